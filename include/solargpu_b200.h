@@ -1,0 +1,161 @@
+/*
+ * solargpu_b200.h -- C ABI of libsolargpu_b200.so, a B200 (sm_100a) build of
+ * SolarGPU's annual DSM irradiance path: DDA viewshed tracer, shadowed
+ * direct + Perez diffuse pass, and the inter-reflection pass over CSR or
+ * ba-RLE neighbor lists.
+ *
+ * Reference interfaces replaced (paths relative to the SolarGPU tree):
+ *   solar_gpu_uncompressed_gpu_irradiance  <- solar_gpu::uncompressed_gpu_irradiance,
+ *                                             include/solar_gpu_api.h:37-42
+ *   solar_gpu_compressed_gpu_irradiance    <- solar_gpu::compressed_gpu_irradiance,
+ *                                             include/solar_gpu_api.h:49-54
+ * The library also exports those two C++ symbols themselves (namespace
+ * solar_gpu, identical signatures), so the reference CLI links against it
+ * unchanged; they forward to the C functions below.
+ *
+ * Plain C: pointers, sizes and ints only.  All functions return 0 on success
+ * and a negative SOLAR_GPU_ERR_* code otherwise (the reference exits the
+ * process on a CUDA error instead); solar_gpu_last_error() describes the
+ * last failure of the calling thread.
+ */
+#ifndef SOLARGPU_B200_H
+#define SOLARGPU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOLAR_GPU_HOURS_PER_YEAR 8760   /* include/pipeline_constants.h:10 */
+
+enum {
+    SOLAR_GPU_OK = 0,
+    SOLAR_GPU_ERR_ARG = -1,          /* bad argument: null pointer, size, option, index range */
+    SOLAR_GPU_ERR_CUDA = -2,         /* a CUDA runtime call or kernel launch failed */
+    SOLAR_GPU_ERR_NO_DEVICE = -3,    /* no usable CUDA device */
+    SOLAR_GPU_ERR_OOM = -4,          /* device allocation failed */
+    SOLAR_GPU_ERR_DEVICE_CHECK = -5  /* a kernel flagged malformed data (e.g. a ba-RLE stream) */
+};
+
+/* Neighbor list storage (reference: the two pipeline instances). */
+enum { SOLAR_GPU_CSR = 0, SOLAR_GPU_BARLE = 1, SOLAR_GPU_BOTH = 2 };
+/* Annual accumulation. */
+enum { SOLAR_GPU_ACC_FP64 = 0, SOLAR_GPU_ACC_KAHAN = 1, SOLAR_GPU_ACC_FP32 = 2 };
+/* Reflection evaluation. */
+enum { SOLAR_GPU_REFL_HOURLY = 0, SOLAR_GPU_REFL_ANNUAL = 1 };
+
+typedef struct solar_gpu_options {
+    int neighbor_format;     /* SOLAR_GPU_CSR / SOLAR_GPU_BARLE (SOLAR_GPU_BOTH: trace only) */
+    int hour_block;          /* 1 = plain per-hour path; 32, 64, 128, 256 = hour-block SpMM width; 0 = default (128) */
+    int accumulation;        /* SOLAR_GPU_ACC_* */
+    int reflection;          /* SOLAR_GPU_REFL_HOURLY (reflection per hour, reference semantics) or
+                                SOLAR_GPU_REFL_ANNUAL (sum over hours first, one sparse product) */
+    long long chunk_voxels;  /* tracer chunk in voxels (bounds the raw hit buffer); 0 = from free memory */
+    int use_graph;           /* capture the hour-block loop in a CUDA graph */
+} solar_gpu_options;
+
+void solar_gpu_default_options(solar_gpu_options* opt);
+
+/* ---- drop-in entry points (synchronous, host buffers, device 0) -------- */
+
+/* Same arguments as the reference (include/solar_gpu_api.h:15-36); the
+   std::vector arguments become pointer + count.  As in the reference only
+   the first 8760 entries of each series are used; a count below 8760 is
+   SOLAR_GPU_ERR_ARG.  sun_positions is [8760][2] (azimuth_deg, altitude_deg).  wall_z may
+   be NULL when num_total_voxels == num_top_voxels.  irradiance_out receives
+   num_total_voxels annual sums (Wh/m^2). */
+int solar_gpu_uncompressed_gpu_irradiance(
+    const float* grid_data, int grid_width, int grid_height,
+    int num_total_voxels, int num_top_voxels,
+    const int* pixel_parent, const float* wall_z, float max_height,
+    const float* sun_positions, int num_sun_positions,
+    const float* direct_irradiance, int num_direct,
+    const float* diffuse_irradiance, int num_diffuse,
+    const float* slopes, const float* aspects, float* irradiance_out);
+
+int solar_gpu_compressed_gpu_irradiance(
+    const float* grid_data, int grid_width, int grid_height,
+    int num_total_voxels, int num_top_voxels,
+    const int* pixel_parent, const float* wall_z, float max_height,
+    const float* sun_positions, int num_sun_positions,
+    const float* direct_irradiance, int num_direct,
+    const float* diffuse_irradiance, int num_diffuse,
+    const float* slopes, const float* aspects, float* irradiance_out);
+
+/* ---- context API: persistent device workspace and stream --------------- */
+
+typedef struct solar_gpu_context solar_gpu_context;
+
+int solar_gpu_create(int device, solar_gpu_context** out);
+void solar_gpu_destroy(solar_gpu_context* ctx);
+
+/* Scene description.  For solar_gpu_run_host the array pointers are host
+   pointers; for solar_gpu_run_device and solar_gpu_trace the per-cell and
+   per-voxel arrays (grid, pixel_parent, wall_z, slopes, aspects) are device
+   pointers while the 8760-entry series (sun_positions, direct, diffuse)
+   stay host pointers. */
+typedef struct solar_gpu_scene {
+    const float* grid;
+    int grid_width, grid_height;
+    int num_total_voxels, num_top_voxels;
+    const int* pixel_parent;
+    const float* wall_z;
+    float max_height;
+    const float* sun_positions;     /* [8760][2] host */
+    const float* direct_irradiance; /* [8760] host */
+    const float* diffuse_irradiance;/* [8760] host */
+    const float* slopes;
+    const float* aspects;
+} solar_gpu_scene;
+
+/* Host buffers in and out; copies, compute and the read-back are inside. */
+int solar_gpu_run_host(solar_gpu_context* ctx, const solar_gpu_options* opt,
+                       const solar_gpu_scene* scene, float* irradiance_out);
+
+/* Device-resident inputs and output, enqueued on `stream` (cudaStream_t or
+   NULL for the context's own stream).  Returns after the work is enqueued
+   except for the small host synchronisations Stage 1 needs to size its
+   output buffers. */
+int solar_gpu_run_device(solar_gpu_context* ctx, const solar_gpu_options* opt,
+                         const solar_gpu_scene* scene, float* irradiance_out_device,
+                         void* stream);
+
+/* ---- stage access (parity checks, tools) ------------------------------- */
+
+/* Runs Stage 1 only (device scene), building the lists opt->neighbor_format
+   asks for (SOLAR_GPU_BOTH builds both).  Synchronous. */
+int solar_gpu_trace(solar_gpu_context* ctx, const solar_gpu_options* opt,
+                    const solar_gpu_scene* scene, void* stream);
+
+/* Sizes of the last Stage 1 result. */
+int solar_gpu_trace_sizes(solar_gpu_context* ctx, long long* csr_entries, long long* barle_bytes,
+                          int* shadow_words, int* active_bins, int* num_voxels);
+
+/* Copies the last Stage 1 result to host buffers (any may be NULL):
+   csr_offsets [N+1] int64, csr_ids [csr_entries] (1-based cell ids in
+   first-hit direction order, as the reference CSR), barle_offsets [N+1],
+   barle_bytes [barle_bytes] (byte-identical to the reference encoder),
+   shadow [N][shadow_words] uint32 (bit b of word w set = dense sun bin 32w+b
+   is blocked for that voxel). */
+int solar_gpu_trace_copy(solar_gpu_context* ctx, long long* csr_offsets, int* csr_ids,
+                         long long* barle_offsets, unsigned char* barle_bytes, uint32_t* shadow);
+
+/* Stage times of the last run, milliseconds, from CUDA events:
+   [0] setup (tables, geometry), [1] Stage 1 (trace + lists),
+   [2] Stage 2/3 (solar + reflection + accumulation), [3] total.
+   Returns the number of values written. */
+int solar_gpu_last_timings(solar_gpu_context* ctx, double* ms, int n);
+
+/* Number of kernel launches the library issued in the last run. */
+long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* solar_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOLARGPU_B200_H */

@@ -1,0 +1,263 @@
+"""Python front end of libsolargpu_b200.so (ctypes over the C ABI in
+include/solargpu_b200.h).
+
+``uncompressed_gpu_irradiance`` / ``compressed_gpu_irradiance`` mirror the
+reference entry points (include/solar_gpu_api.h:37-54) argument for
+argument: host arrays in, the annual irradiance written into
+``irradiance_out``, 0 returned on success.  Where the reference would exit
+the process on a CUDA error, these raise :class:`SolarGPUError`.
+
+:class:`Context` exposes the rest of the ABI: device-resident runs on a
+caller stream, Stage 1 results for parity checks, stage timings.
+
+The library is the only compute path: if it is missing or no GPU is
+present, calls raise; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libsolargpu_b200.so")
+HOURS_PER_YEAR = 8760
+
+CSR, BARLE, BOTH = 0, 1, 2
+ACC_FP64, ACC_KAHAN, ACC_FP32 = 0, 1, 2
+REFL_HOURLY, REFL_ANNUAL = 0, 1
+
+_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no CUDA device",
+           -4: "out of device memory", -5: "device data check failed"}
+
+
+class SolarGPUError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRORS.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [("neighbor_format", C.c_int), ("hour_block", C.c_int), ("accumulation", C.c_int),
+                ("reflection", C.c_int), ("chunk_voxels", C.c_longlong), ("use_graph", C.c_int)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("grid", C.c_void_p), ("grid_width", C.c_int), ("grid_height", C.c_int),
+                ("num_total_voxels", C.c_int), ("num_top_voxels", C.c_int),
+                ("pixel_parent", C.c_void_p), ("wall_z", C.c_void_p), ("max_height", C.c_float),
+                ("sun_positions", C.c_void_p), ("direct_irradiance", C.c_void_p),
+                ("diffuse_irradiance", C.c_void_p), ("slopes", C.c_void_p), ("aspects", C.c_void_p)]
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """Loads the CUDA library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise SolarGPUError(-3, f"{LIB_PATH} is missing; build it with `python -m solargpu_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, i, f, ll = C.c_void_p, C.c_int, C.c_float, C.c_longlong
+        L.solar_gpu_last_error.restype = C.c_char_p
+        L.solar_gpu_last_launch_count.restype = ll
+        L.solar_gpu_last_launch_count.argtypes = [vp]
+        for name in ("solar_gpu_uncompressed_gpu_irradiance", "solar_gpu_compressed_gpu_irradiance"):
+            fn = getattr(L, name)
+            fn.argtypes = [vp, i, i, i, i, vp, vp, f, vp, i, vp, i, vp, i, vp, vp, vp]
+            fn.restype = i
+        L.solar_gpu_create.argtypes = [i, C.POINTER(vp)]
+        L.solar_gpu_destroy.argtypes = [vp]
+        L.solar_gpu_destroy.restype = None
+        L.solar_gpu_default_options.argtypes = [C.POINTER(Options)]
+        L.solar_gpu_default_options.restype = None
+        L.solar_gpu_run_host.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), vp]
+        L.solar_gpu_run_device.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), vp, vp]
+        L.solar_gpu_trace.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), vp]
+        L.solar_gpu_trace_sizes.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+        L.solar_gpu_trace_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.solar_gpu_last_timings.argtypes = [vp, C.POINTER(C.c_double), i]
+        _LIB = L
+    return _LIB
+
+
+def _check(rc: int) -> int:
+    if rc != 0:
+        raise SolarGPUError(rc, lib().solar_gpu_last_error().decode(errors="replace"))
+    return rc
+
+
+def _host(a, dtype) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _p(a) -> int | None:
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return int(a.data_ptr())
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a)
+
+
+def options(**kw) -> Options:
+    o = Options()
+    lib().solar_gpu_default_options(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+# ---------------------------------------------------------------- drop-in mirror
+
+def _drop_in(compressed, grid_data, grid_width, grid_height, num_total_voxels, num_top_voxels,
+             pixel_parent, wall_z, max_height, sun_positions, direct_irradiance, diffuse_irradiance,
+             slopes, aspects, irradiance_out):
+    grid = _host(grid_data, np.float32)
+    pp = _host(pixel_parent, np.int32)
+    wz = None if wall_z is None or np.size(wall_z) == 0 else _host(wall_z, np.float32)
+    sun = _host(sun_positions, np.float32).reshape(-1, 2)
+    dn = _host(direct_irradiance, np.float32)
+    df = _host(diffuse_irradiance, np.float32)
+    sl = _host(slopes, np.float32)
+    asp = _host(aspects, np.float32)
+    if not (isinstance(irradiance_out, np.ndarray) and irradiance_out.dtype == np.float32
+            and irradiance_out.flags.c_contiguous and irradiance_out.size >= num_total_voxels):
+        raise TypeError("irradiance_out must be a contiguous float32 array of num_total_voxels")
+    fn = lib().solar_gpu_compressed_gpu_irradiance if compressed else lib().solar_gpu_uncompressed_gpu_irradiance
+    return _check(fn(_p(grid), grid_width, grid_height, num_total_voxels, num_top_voxels, _p(pp), _p(wz),
+                     float(max_height), _p(sun), sun.shape[0], _p(dn), dn.size, _p(df), df.size,
+                     _p(sl), _p(asp), _p(irradiance_out)))
+
+
+def uncompressed_gpu_irradiance(grid_data, grid_width, grid_height, num_total_voxels, num_top_voxels,
+                                pixel_parent, wall_z, max_height, sun_positions, direct_irradiance,
+                                diffuse_irradiance, slopes, aspects, irradiance_out) -> int:
+    """Annual irradiance with CSR neighbor lists (include/solar_gpu_api.h:37-42)."""
+    return _drop_in(False, grid_data, grid_width, grid_height, num_total_voxels, num_top_voxels,
+                    pixel_parent, wall_z, max_height, sun_positions, direct_irradiance,
+                    diffuse_irradiance, slopes, aspects, irradiance_out)
+
+
+def compressed_gpu_irradiance(grid_data, grid_width, grid_height, num_total_voxels, num_top_voxels,
+                              pixel_parent, wall_z, max_height, sun_positions, direct_irradiance,
+                              diffuse_irradiance, slopes, aspects, irradiance_out) -> int:
+    """Annual irradiance with ba-RLE neighbor lists decoded on the fly
+    (include/solar_gpu_api.h:49-54)."""
+    return _drop_in(True, grid_data, grid_width, grid_height, num_total_voxels, num_top_voxels,
+                    pixel_parent, wall_z, max_height, sun_positions, direct_irradiance,
+                    diffuse_irradiance, slopes, aspects, irradiance_out)
+
+
+# ---------------------------------------------------------------- context
+
+def _scene_desc(scene, dev: dict | None = None) -> tuple[SceneDesc, list]:
+    """Builds the C scene struct.  With `dev`, the per-voxel arrays come from
+    device tensors (dict with grid, pixel_parent, wall_z, slopes, aspects)."""
+    keep = []
+    d = SceneDesc()
+    d.grid_width = scene.width
+    d.grid_height = scene.height
+    d.num_total_voxels = scene.num_total
+    d.num_top_voxels = scene.num_top
+    d.max_height = scene.max_height
+    for name, dt in (("sun", np.float32), ("direct", np.float32), ("diffuse", np.float32)):
+        a = _host(getattr(scene, name), dt)
+        keep.append(a)
+    d.sun_positions, d.direct_irradiance, d.diffuse_irradiance = (_p(a) for a in keep[-3:])
+    src = dev if dev is not None else {
+        "grid": _host(scene.grid, np.float32), "pixel_parent": _host(scene.pixel_parent, np.int32),
+        "wall_z": _host(scene.wall_z, np.float32) if scene.wall_z.size else None,
+        "slopes": _host(scene.slopes, np.float32), "aspects": _host(scene.aspects, np.float32)}
+    keep.append(src)
+    d.grid = _p(src["grid"])
+    d.pixel_parent = _p(src["pixel_parent"])
+    wz = src.get("wall_z")
+    d.wall_z = _p(wz) if wz is not None and (getattr(wz, "numel", lambda: np.size(wz))() > 0) else None
+    d.slopes = _p(src["slopes"])
+    d.aspects = _p(src["aspects"])
+    return d, keep
+
+
+class Context:
+    """A device workspace + stream (solar_gpu_create / solar_gpu_destroy)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().solar_gpu_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().solar_gpu_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_host(self, scene, out: np.ndarray | None = None, **opts) -> np.ndarray:
+        """Host arrays in and out (copies and read-back inside the call)."""
+        o = options(**opts)
+        d, keep = _scene_desc(scene)
+        if out is None:
+            out = np.zeros(scene.num_total, np.float32)
+        _check(lib().solar_gpu_run_host(self.h, C.byref(o), C.byref(d), _p(out)))
+        return out
+
+    def run_device(self, scene, dev: dict, out, stream=None, **opts) -> None:
+        """Device-resident arrays (`dev`, e.g. torch CUDA tensors) and output."""
+        o = options(**opts)
+        d, keep = _scene_desc(scene, dev)
+        _check(lib().solar_gpu_run_device(self.h, C.byref(o), C.byref(d), _p(out), stream))
+
+    def trace(self, scene, dev: dict, neighbor_format: int = BOTH, stream=None, **opts) -> dict:
+        """Runs Stage 1 and returns its lists and shadow words as numpy arrays."""
+        o = options(neighbor_format=neighbor_format, **opts)
+        d, keep = _scene_desc(scene, dev)
+        _check(lib().solar_gpu_trace(self.h, C.byref(o), C.byref(d), stream))
+        ne, nb = C.c_longlong(), C.c_longlong()
+        w, a, n = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().solar_gpu_trace_sizes(self.h, C.byref(ne), C.byref(nb), C.byref(w), C.byref(a), C.byref(n)))
+        N = n.value
+        res = {"shadow_words": w.value, "active_bins": a.value}
+        csr_off = csr_ids = b_off = b_bytes = None
+        if ne.value >= 0:
+            csr_off = np.zeros(N + 1, np.int64)
+            csr_ids = np.zeros(max(1, ne.value), np.int32)
+        if nb.value >= 0:
+            b_off = np.zeros(N + 1, np.int64)
+            b_bytes = np.zeros(max(1, nb.value), np.uint8)
+        shadow = np.zeros((N, w.value), np.uint32)
+        _check(lib().solar_gpu_trace_copy(self.h, _p(csr_off), _p(csr_ids), _p(b_off), _p(b_bytes), _p(shadow)))
+        if csr_off is not None:
+            res["csr_off"], res["csr_ids"] = csr_off, csr_ids[:ne.value]
+        if b_off is not None:
+            res["barle_off"], res["barle"] = b_off, b_bytes[:nb.value]
+        res["shadow"] = shadow
+        return res
+
+    def timings(self) -> list[float]:
+        """[setup, stage 1, stage 2/3, total] of the last run, ms (CUDA events)."""
+        ms = (C.c_double * 4)()
+        n = lib().solar_gpu_last_timings(self.h, ms, 4)
+        if n < 0:
+            _check(n)
+        return list(ms)[:n]
+
+    def launches(self) -> int:
+        return int(lib().solar_gpu_last_launch_count(self.h))

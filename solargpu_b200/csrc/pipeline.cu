@@ -1,0 +1,617 @@
+// Host orchestration and the C ABI (include/solargpu_b200.h).
+//
+// Replaces the reference pipeline hosts (src/cuda/gpu_irradiance_uncompressed.cu,
+// src/cuda/gpu_irradiance_compressed.cu) and the out-of-core viewshed driver
+// (include/cuda/viewshed_stage.cuh:37-125):
+//   * all state lives in a context (no __constant__ globals), so calls are
+//     reentrant per context and run on the caller's stream;
+//   * device buffers are grow-only and reused across calls;
+//   * Stage 1 runs in voxel chunks bounded by a memory budget, and builds the
+//     CSR and/or ba-RLE lists on the device (no host round trip of the raw
+//     hit buffer, no host encoder);
+//   * errors come back as return codes, never exit().
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "solargpu_b200.h"
+#include "sgb_internal.cuh"
+#include "sky.h"
+
+using namespace sgb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what, int line)
+{
+    const int code = (e == cudaErrorMemoryAllocation) ? SOLAR_GPU_ERR_OOM
+                   : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? SOLAR_GPU_ERR_NO_DEVICE
+                   : SOLAR_GPU_ERR_CUDA;
+    cudaGetLastError();   // clear a sticky launch error so the context stays usable
+    return fail(code, "%s failed (pipeline.cu:%d): %s", what, line, cudaGetErrorString(e));
+}
+
+#define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return cuda_fail(e_, #call, __LINE__); } while (0)
+#define RK(call) do { int r_ = (call); if (r_ != SOLAR_GPU_OK) return r_; } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+template <typename T> T* as(DevBuf& b) { return static_cast<T*>(b.p); }
+
+__global__ void k_validate_parents(const int* __restrict__ pp, int N, int T, int* __restrict__ bad)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const int p = pp[v];
+    // Layout contract of src/main.cpp:112-127: tops are cells in raster order.
+    if ((v < T && p != v) || p < 0 || p >= T) atomicOr(bad, 1);
+}
+
+}  // namespace
+
+struct solar_gpu_context {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaEvent_t ev[4] = {};
+    DevBuf dirs, nudged, dni, dhi, sun_dense, hour_index, table, geo_n, geo_p, shadow, raw,
+        counts, csr_off, csr_ids, barle_off, barle_sizes, barle_bytes, scan_tmp, slab, hourly,
+        acc_f64, acc_f32, acc_comp, sums, out_f64, err, in_grid, in_pp, in_wz, in_slopes,
+        in_aspects, out_f32;
+    int* h_scalars = nullptr;   // pinned host scratch for small read-backs
+    // last Stage 1 result
+    int N = 0, T = 0, words32 = 0, active = 0;
+    long long csr_total = 0, barle_total = 0;
+    bool have_csr = false, have_barle = false;
+    double timings[4] = {0, 0, 0, 0};
+    long long launches = 0;
+    bool timed = false;
+};
+
+namespace {
+
+int ensure(DevBuf& b, size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return SOLAR_GPU_OK;
+    if (b.p) CK(cudaFree(b.p));
+    b.p = nullptr;
+    b.cap = 0;
+    const size_t cap = (bytes + 255) & ~(size_t)255;
+    CK(cudaMalloc(&b.p, cap));
+    b.cap = cap;
+    return SOLAR_GPU_OK;
+}
+
+// Grows `b` to at least `bytes`, keeping the first `used` bytes.
+int ensure_keep(DevBuf& b, size_t bytes, size_t used, cudaStream_t st)
+{
+    if (b.cap >= bytes) return SOLAR_GPU_OK;
+    void* np = nullptr;
+    const size_t cap = ((bytes + bytes / 8) + 255) & ~(size_t)255;
+    CK(cudaMalloc(&np, cap));
+    if (used && b.p) CK(cudaMemcpyAsync(np, b.p, used, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    if (b.p) CK(cudaFree(b.p));
+    b.p = np;
+    b.cap = cap;
+    return SOLAR_GPU_OK;
+}
+
+int read_ll(solar_gpu_context* c, const long long* dev, long long* out, cudaStream_t st)
+{
+    CK(cudaMemcpyAsync(c->h_scalars, dev, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::memcpy(out, c->h_scalars, sizeof(long long));
+    return SOLAR_GPU_OK;
+}
+
+int check_scene(const solar_gpu_scene* s)
+{
+    if (!s) return fail(SOLAR_GPU_ERR_ARG, "scene is NULL");
+    if (s->grid_width <= 0 || s->grid_height <= 0)
+        return fail(SOLAR_GPU_ERR_ARG, "grid size %dx%d", s->grid_width, s->grid_height);
+    if ((long long)s->grid_width * s->grid_height != (long long)s->num_top_voxels)
+        return fail(SOLAR_GPU_ERR_ARG, "num_top_voxels %d != grid_width * grid_height", s->num_top_voxels);
+    if (s->num_total_voxels < s->num_top_voxels)
+        return fail(SOLAR_GPU_ERR_ARG, "num_total_voxels %d < num_top_voxels", s->num_total_voxels);
+    if (!s->grid || !s->pixel_parent || !s->slopes || !s->aspects)
+        return fail(SOLAR_GPU_ERR_ARG, "a voxel array pointer is NULL");
+    if (s->num_total_voxels > s->num_top_voxels && !s->wall_z)
+        return fail(SOLAR_GPU_ERR_ARG, "wall_z is NULL but there are %d wall voxels",
+                    s->num_total_voxels - s->num_top_voxels);
+    if (!s->sun_positions || !s->direct_irradiance || !s->diffuse_irradiance)
+        return fail(SOLAR_GPU_ERR_ARG, "an hourly series pointer is NULL");
+    return SOLAR_GPU_OK;
+}
+
+int check_options(const solar_gpu_options* o, bool trace_only)
+{
+    if (!o) return fail(SOLAR_GPU_ERR_ARG, "options is NULL");
+    if (o->neighbor_format < 0 || o->neighbor_format > 2 || (!trace_only && o->neighbor_format == 2))
+        return fail(SOLAR_GPU_ERR_ARG, "neighbor_format %d", o->neighbor_format);
+    const int B = o->hour_block;
+    if (!(B == 0 || B == 1 || B == 32 || B == 64 || B == 128 || B == 256))
+        return fail(SOLAR_GPU_ERR_ARG, "hour_block %d (1, 32, 64, 128 or 256)", B);
+    if (o->accumulation < 0 || o->accumulation > 2) return fail(SOLAR_GPU_ERR_ARG, "accumulation %d", o->accumulation);
+    if (o->reflection < 0 || o->reflection > 1) return fail(SOLAR_GPU_ERR_ARG, "reflection %d", o->reflection);
+    if (o->chunk_voxels < 0) return fail(SOLAR_GPU_ERR_ARG, "chunk_voxels %lld", o->chunk_voxels);
+    return SOLAR_GPU_OK;
+}
+
+DevScene dev_scene(const solar_gpu_scene* s)
+{
+    DevScene d;
+    d.grid = s->grid;
+    d.pix_parent = s->pixel_parent;
+    d.wall_z = s->wall_z;
+    d.slopes = s->slopes;
+    d.aspects = s->aspects;
+    d.W = s->grid_width;
+    d.H = s->grid_height;
+    d.N = s->num_total_voxels;
+    d.T = s->num_top_voxels;
+    d.maxz = s->max_height;
+    return d;
+}
+
+// Tables, geometry and input validation.
+int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cudaStream_t st)
+{
+    sky = make_sky_tables(s->sun_positions);
+    const int D = (int)sky.dirs.size();
+    const int Hd = (int)sky.hour_index.size();
+    const int n_padded = ((Hd + 255) / 256) * 256 + 256;
+    RK(ensure(c->dirs, sizeof(DirEntry) * D));
+    RK(ensure(c->nudged, sizeof(float) * 2 * kHoursPerYear));
+    RK(ensure(c->dni, sizeof(float) * kHoursPerYear));
+    RK(ensure(c->dhi, sizeof(float) * kHoursPerYear));
+    RK(ensure(c->sun_dense, sizeof(int) * kHoursPerYear));
+    RK(ensure(c->hour_index, sizeof(int) * (Hd + 1)));
+    RK(ensure(c->table, sizeof(HourEntry) * n_padded));
+    RK(ensure(c->err, sizeof(int)));
+    CK(cudaMemcpyAsync(c->dirs.p, sky.dirs.data(), sizeof(DirEntry) * D, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->nudged.p, sky.nudged.data(), sizeof(float) * 2 * kHoursPerYear, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->dni.p, s->direct_irradiance, sizeof(float) * kHoursPerYear, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->dhi.p, s->diffuse_irradiance, sizeof(float) * kHoursPerYear, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->sun_dense.p, sky.sun_dense.data(), sizeof(int) * kHoursPerYear, cudaMemcpyHostToDevice, st));
+    if (Hd) CK(cudaMemcpyAsync(c->hour_index.p, sky.hour_index.data(), sizeof(int) * Hd, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(c->err.p, 0, sizeof(int), st));
+    CK(launch_hour_table(as<float>(c->nudged), as<float>(c->dni), as<float>(c->dhi), as<int>(c->sun_dense),
+                         as<int>(c->hour_index), Hd, n_padded, as<HourEntry>(c->table), st));
+    const int N = s->num_total_voxels;
+    RK(ensure(c->geo_n, sizeof(float4) * (size_t)N));
+    RK(ensure(c->geo_p, sizeof(float4) * (size_t)N));
+    k_validate_parents<<<(N + 255) / 256, 256, 0, st>>>(s->pixel_parent, N, s->num_top_voxels, as<int>(c->err));
+    CK(cudaGetLastError());
+    int bad = 0;
+    CK(cudaMemcpyAsync(c->h_scalars, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::memcpy(&bad, c->h_scalars, sizeof(int));
+    if (bad) return fail(SOLAR_GPU_ERR_ARG, "pixel_parent violates the voxel layout (tops i -> i, walls in [0, T))");
+    DevGeom g{as<float4>(c->geo_n), as<float4>(c->geo_p)};
+    CK(launch_voxel_geom(dev_scene(s), g, st));
+    c->launches += 3;
+    return SOLAR_GPU_OK;
+}
+
+long long auto_chunk(int N, int D)
+{
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
+    // The raw hit rows (D ints per voxel) get at most 35 % of free memory.
+    const double budget = 0.35 * (double)free_b;
+    long long chunk = (long long)(budget / ((double)D * sizeof(int)));
+    if (chunk < 1024) chunk = 1024;
+    if (chunk > N) chunk = N;
+    return chunk;
+}
+
+int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
+           const SkyTables& sky, cudaStream_t st, bool want_csr, bool want_barle)
+{
+    const int N = s->num_total_voxels;
+    const int D = (int)sky.dirs.size();
+    const long long chunk = o->chunk_voxels > 0 ? (o->chunk_voxels < N ? o->chunk_voxels : N) : auto_chunk(N, D);
+    c->N = N;
+    c->T = s->num_top_voxels;
+    c->words32 = sky.words32 > 0 ? sky.words32 : 1;
+    c->active = sky.active;
+    c->have_csr = want_csr;
+    c->have_barle = want_barle;
+    c->csr_total = c->barle_total = 0;
+    RK(ensure(c->shadow, sizeof(uint32_t) * (size_t)N * c->words32));
+    CK(cudaMemsetAsync(c->shadow.p, 0, sizeof(uint32_t) * (size_t)N * c->words32, st));
+    RK(ensure(c->raw, sizeof(int) * (size_t)chunk * D));
+    RK(ensure(c->counts, sizeof(int) * (size_t)N));
+    RK(ensure(c->scan_tmp, sizeof(long long) * scan_scratch_elems((int)chunk)));
+    if (want_csr) {
+        RK(ensure(c->csr_off, sizeof(long long) * ((size_t)N + 1)));
+        RK(ensure(c->csr_ids, sizeof(int) * (size_t)N * 96));
+    }
+    if (want_barle) {
+        RK(ensure(c->barle_off, sizeof(long long) * ((size_t)N + 1)));
+        RK(ensure(c->barle_sizes, sizeof(int) * (size_t)N));
+        RK(ensure(c->barle_bytes, (size_t)N * 160));
+    }
+    const DevScene ds = dev_scene(s);
+    long long csr_total = 0, barle_total = 0;
+    for (long long v0 = 0; v0 < N; v0 += chunk) {
+        const int n = (int)((N - v0) < chunk ? (N - v0) : chunk);
+        CK(launch_trace(ds, as<DirEntry>(c->dirs), D, c->words32, (int)v0, n, as<int>(c->raw),
+                        as<uint32_t>(c->shadow), st));
+        CK(launch_dedupe(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->err), st));
+        c->launches += 2;
+        const double frac_left = (double)N / (double)(v0 + n);
+        if (want_csr) {
+            long long* off = as<long long>(c->csr_off) + v0;
+            CK(launch_scan_counts(as<int>(c->counts) + v0, n, csr_total, off, as<long long>(c->scan_tmp), nullptr, st));
+            long long total = 0;
+            RK(read_ll(c, off + n, &total, st));
+            const long long est = (long long)(total * frac_left * 1.05);
+            RK(ensure_keep(c->csr_ids, sizeof(int) * (size_t)(est > total ? est : total), sizeof(int) * (size_t)csr_total, st));
+            CK(launch_gather_csr(n, D, as<int>(c->raw), off, as<int>(c->csr_ids), st));
+            csr_total = total;
+            c->launches += 4;
+        }
+        if (want_barle) {
+            long long* off = as<long long>(c->barle_off) + v0;
+            CK(launch_barle_size(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->barle_sizes) + v0,
+                                 as<int>(c->err), st));
+            CK(launch_scan_counts(as<int>(c->barle_sizes) + v0, n, barle_total, off, as<long long>(c->scan_tmp), nullptr, st));
+            long long total = 0;
+            RK(read_ll(c, off + n, &total, st));
+            const long long est = (long long)(total * frac_left * 1.05);
+            RK(ensure_keep(c->barle_bytes, (size_t)(est > total ? est : total), (size_t)barle_total, st));
+            CK(launch_barle_write(n, D, as<int>(c->raw), as<int>(c->counts) + v0, off,
+                                  as<unsigned char>(c->barle_bytes), as<int>(c->err), st));
+            barle_total = total;
+            c->launches += 5;
+        }
+    }
+    c->csr_total = csr_total;
+    c->barle_total = barle_total;
+    return SOLAR_GPU_OK;
+}
+
+int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
+            const SkyTables& sky, float* out, cudaStream_t st)
+{
+    const int N = s->num_total_voxels, T = s->num_top_voxels;
+    const int Hd = (int)sky.hour_index.size();
+    const int B = o->hour_block == 0 ? 128 : o->hour_block;
+    DevGeom g{as<float4>(c->geo_n), as<float4>(c->geo_p)};
+    NeighborLists nl;
+    nl.format = o->neighbor_format;
+    if (nl.format == SOLAR_GPU_CSR) {
+        nl.offsets = as<long long>(c->csr_off);
+        nl.ids = as<int>(c->csr_ids);
+        nl.bytes = nullptr;
+    } else {
+        nl.offsets = as<long long>(c->barle_off);
+        nl.ids = nullptr;
+        nl.bytes = as<unsigned char>(c->barle_bytes);
+    }
+    const uint32_t* sh = as<uint32_t>(c->shadow);
+    const HourEntry* tab = as<HourEntry>(c->table);
+    int* err = as<int>(c->err);
+    if (o->reflection == SOLAR_GPU_REFL_ANNUAL) {
+        RK(ensure(c->sums, sizeof(double) * (size_t)N));
+        RK(ensure(c->out_f64, sizeof(double) * (size_t)N));
+        CK(launch_solar_sum(g, N, sh, c->words32, tab, Hd, as<double>(c->sums), st));
+        CK(launch_reflect_annual(g, N, T, as<double>(c->sums), nl, as<double>(c->out_f64), err, st));
+        CK(launch_finalize_f64(as<double>(c->out_f64), N, out, st));
+        c->launches += 3;
+        return SOLAR_GPU_OK;
+    }
+    Accum acc;
+    acc.mode = o->accumulation;
+    acc.f64 = nullptr;
+    acc.f32 = acc.comp = nullptr;
+    if (acc.mode == SOLAR_GPU_ACC_FP64) {
+        RK(ensure(c->acc_f64, sizeof(double) * (size_t)N));
+        acc.f64 = as<double>(c->acc_f64);
+        CK(cudaMemsetAsync(acc.f64, 0, sizeof(double) * (size_t)N, st));
+    } else {
+        RK(ensure(c->acc_f32, sizeof(float) * (size_t)N));
+        RK(ensure(c->acc_comp, sizeof(float) * (size_t)N));
+        acc.f32 = as<float>(c->acc_f32);
+        acc.comp = as<float>(c->acc_comp);
+        CK(cudaMemsetAsync(acc.f32, 0, sizeof(float) * (size_t)N, st));
+        CK(cudaMemsetAsync(acc.comp, 0, sizeof(float) * (size_t)N, st));
+    }
+    if (B == 1) {
+        RK(ensure(c->hourly, sizeof(float) * (size_t)N));
+        for (int j = 0; j < Hd; ++j) {
+            CK(launch_solar_hour(g, N, sh, c->words32, tab, j, as<float>(c->hourly), st));
+            CK(launch_reflect_hour(g, N, T, as<float>(c->hourly), nl, acc, err, st));
+        }
+        c->launches += 2LL * Hd;
+    } else {
+        RK(ensure(c->slab, sizeof(float) * (size_t)T * B));
+        float* slab = as<float>(c->slab);
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        const bool use_graph = o->use_graph != 0;
+        if (use_graph) CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t le = cudaSuccess;
+        for (int j0 = 0; j0 < Hd && le == cudaSuccess; j0 += B) {
+            le = launch_solar_slab(g, T, sh, c->words32, tab, j0, B, slab, st);
+            if (le == cudaSuccess)
+                le = launch_reflect_block(g, N, T, sh, c->words32, tab, j0, B, slab, nl, acc, err, st);
+            c->launches += 2;
+        }
+        if (use_graph) {
+            const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            if (le == cudaSuccess) le = ce;
+            if (le == cudaSuccess) le = cudaGraphInstantiate(&exec, graph, 0);
+            if (le == cudaSuccess) le = cudaGraphLaunch(exec, st);
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+        }
+        CK(le);
+    }
+    CK(launch_finalize(acc, N, out, st));
+    c->launches += 1;
+    return SOLAR_GPU_OK;
+}
+
+int check_device_flags(solar_gpu_context* c, cudaStream_t st)
+{
+    CK(cudaMemcpyAsync(c->h_scalars, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int f = 0;
+    std::memcpy(&f, c->h_scalars, sizeof(int));
+    if (f) return fail(SOLAR_GPU_ERR_DEVICE_CHECK, "device check flags 0x%x (1 = ba-RLE stream, 2 = hash, 4 = capacity)", f);
+    return SOLAR_GPU_OK;
+}
+
+int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
+                    float* out, cudaStream_t st, bool trace_only)
+{
+    RK(check_scene(s));
+    RK(check_options(o, trace_only));
+    if (!trace_only && !out) return fail(SOLAR_GPU_ERR_ARG, "irradiance output is NULL");
+    CK(cudaSetDevice(c->device));
+    c->launches = 0;
+    c->timed = false;
+    CK(cudaEventRecord(c->ev[0], st));
+    SkyTables sky;
+    RK(prepare(c, s, sky, st));
+    CK(cudaEventRecord(c->ev[1], st));
+    const bool csr = o->neighbor_format == SOLAR_GPU_CSR || o->neighbor_format == SOLAR_GPU_BOTH;
+    const bool barle = o->neighbor_format == SOLAR_GPU_BARLE || o->neighbor_format == SOLAR_GPU_BOTH;
+    RK(stage1(c, o, s, sky, st, csr, barle));
+    CK(cudaEventRecord(c->ev[2], st));
+    if (!trace_only) RK(stage23(c, o, s, sky, out, st));
+    CK(cudaEventRecord(c->ev[3], st));
+    c->timed = true;
+    return SOLAR_GPU_OK;
+}
+
+std::mutex g_default_mu;
+solar_gpu_context* g_default = nullptr;
+
+int drop_in(int fmt, const float* grid_data, int grid_width, int grid_height,
+            int num_total_voxels, int num_top_voxels, const int* pixel_parent, const float* wall_z,
+            float max_height, const float* sun_positions, int num_sun, const float* direct, int num_direct,
+            const float* diffuse, int num_diffuse, const float* slopes, const float* aspects, float* out)
+{
+    // The reference reads the first 8760 entries of each series
+    // (src/cuda/device_globals.cu:58-65); fewer is an error here.
+    if (num_sun < kHoursPerYear || num_direct < kHoursPerYear || num_diffuse < kHoursPerYear)
+        return fail(SOLAR_GPU_ERR_ARG, "hourly series need %d entries (got %d, %d, %d)",
+                    kHoursPerYear, num_sun, num_direct, num_diffuse);
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if (!g_default) RK(solar_gpu_create(0, &g_default));
+    solar_gpu_options o;
+    solar_gpu_default_options(&o);
+    o.neighbor_format = fmt;
+    solar_gpu_scene s;
+    s.grid = grid_data;
+    s.grid_width = grid_width;
+    s.grid_height = grid_height;
+    s.num_total_voxels = num_total_voxels;
+    s.num_top_voxels = num_top_voxels;
+    s.pixel_parent = pixel_parent;
+    s.wall_z = wall_z;
+    s.max_height = max_height;
+    s.sun_positions = sun_positions;
+    s.direct_irradiance = direct;
+    s.diffuse_irradiance = diffuse;
+    s.slopes = slopes;
+    s.aspects = aspects;
+    return solar_gpu_run_host(g_default, &o, &s, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+void solar_gpu_default_options(solar_gpu_options* o)
+{
+    if (!o) return;
+    o->neighbor_format = SOLAR_GPU_CSR;
+    o->hour_block = 128;
+    o->accumulation = SOLAR_GPU_ACC_FP64;
+    o->reflection = SOLAR_GPU_REFL_HOURLY;
+    o->chunk_voxels = 0;
+    o->use_graph = 1;
+}
+
+const char* solar_gpu_last_error(void) { return g_err.c_str(); }
+
+int solar_gpu_create(int device, solar_gpu_context** out)
+{
+    if (!out) return fail(SOLAR_GPU_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0) { cudaGetLastError(); return fail(SOLAR_GPU_ERR_NO_DEVICE, "no CUDA device"); }
+    if (device < 0 || device >= n) return fail(SOLAR_GPU_ERR_ARG, "device %d of %d", device, n);
+    CK(cudaSetDevice(device));
+    solar_gpu_context* c = new solar_gpu_context();
+    c->device = device;
+    cudaError_t e1 = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e1 == cudaSuccess; ++i) e1 = cudaEventCreate(&c->ev[i]);
+    if (e1 == cudaSuccess) e1 = cudaMallocHost((void**)&c->h_scalars, 64);
+    if (e1 != cudaSuccess) { solar_gpu_destroy(c); return cuda_fail(e1, "context setup", __LINE__); }
+    *out = c;
+    return SOLAR_GPU_OK;
+}
+
+void solar_gpu_destroy(solar_gpu_context* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->own) cudaStreamSynchronize(c->own);
+    DevBuf* bufs[] = {&c->dirs, &c->nudged, &c->dni, &c->dhi, &c->sun_dense, &c->hour_index, &c->table,
+                      &c->geo_n, &c->geo_p, &c->shadow, &c->raw, &c->counts, &c->csr_off, &c->csr_ids,
+                      &c->barle_off, &c->barle_sizes, &c->barle_bytes, &c->scan_tmp, &c->slab, &c->hourly,
+                      &c->acc_f64, &c->acc_f32, &c->acc_comp, &c->sums, &c->out_f64, &c->err, &c->in_grid,
+                      &c->in_pp, &c->in_wz, &c->in_slopes, &c->in_aspects, &c->out_f32};
+    for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+    for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->own) cudaStreamDestroy(c->own);
+    if (c->h_scalars) cudaFreeHost(c->h_scalars);
+    delete c;
+}
+
+int solar_gpu_run_device(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
+                         float* out, void* stream)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
+    RK(run_device_impl(c, o, s, out, st, false));
+    return check_device_flags(c, st);
+}
+
+int solar_gpu_run_host(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
+                       float* out)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    RK(check_scene(s));
+    if (!out) return fail(SOLAR_GPU_ERR_ARG, "irradiance_out is NULL");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = c->own;
+    const size_t N = (size_t)s->num_total_voxels, T = (size_t)s->num_top_voxels, NW = N - T;
+    RK(ensure(c->in_grid, sizeof(float) * T));
+    RK(ensure(c->in_pp, sizeof(int) * N));
+    RK(ensure(c->in_wz, sizeof(float) * (NW ? NW : 1)));
+    RK(ensure(c->in_slopes, sizeof(float) * N));
+    RK(ensure(c->in_aspects, sizeof(float) * N));
+    RK(ensure(c->out_f32, sizeof(float) * N));
+    CK(cudaMemcpyAsync(c->in_grid.p, s->grid, sizeof(float) * T, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->in_pp.p, s->pixel_parent, sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    if (NW) CK(cudaMemcpyAsync(c->in_wz.p, s->wall_z, sizeof(float) * NW, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->in_slopes.p, s->slopes, sizeof(float) * N, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->in_aspects.p, s->aspects, sizeof(float) * N, cudaMemcpyHostToDevice, st));
+    solar_gpu_scene d = *s;
+    d.grid = as<float>(c->in_grid);
+    d.pixel_parent = as<int>(c->in_pp);
+    d.wall_z = NW ? as<float>(c->in_wz) : nullptr;
+    d.slopes = as<float>(c->in_slopes);
+    d.aspects = as<float>(c->in_aspects);
+    RK(run_device_impl(c, o, &d, as<float>(c->out_f32), st, false));
+    CK(cudaMemcpyAsync(out, c->out_f32.p, sizeof(float) * N, cudaMemcpyDeviceToHost, st));
+    return check_device_flags(c, st);
+}
+
+int solar_gpu_trace(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s, void* stream)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
+    RK(run_device_impl(c, o, s, nullptr, st, true));
+    return check_device_flags(c, st);
+}
+
+int solar_gpu_trace_sizes(solar_gpu_context* c, long long* csr_entries, long long* barle_bytes,
+                          int* shadow_words, int* active_bins, int* num_voxels)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    if (csr_entries) *csr_entries = c->have_csr ? c->csr_total : -1;
+    if (barle_bytes) *barle_bytes = c->have_barle ? c->barle_total : -1;
+    if (shadow_words) *shadow_words = c->words32;
+    if (active_bins) *active_bins = c->active;
+    if (num_voxels) *num_voxels = c->N;
+    return SOLAR_GPU_OK;
+}
+
+int solar_gpu_trace_copy(solar_gpu_context* c, long long* csr_offsets, int* csr_ids,
+                         long long* barle_offsets, unsigned char* barle_bytes, uint32_t* shadow)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    CK(cudaSetDevice(c->device));
+    const size_t N = (size_t)c->N;
+    if ((csr_offsets || csr_ids) && !c->have_csr) return fail(SOLAR_GPU_ERR_ARG, "no CSR lists in the last trace");
+    if ((barle_offsets || barle_bytes) && !c->have_barle) return fail(SOLAR_GPU_ERR_ARG, "no ba-RLE lists in the last trace");
+    CK(cudaStreamSynchronize(c->own));
+    CK(cudaDeviceSynchronize());
+    if (csr_offsets) CK(cudaMemcpy(csr_offsets, c->csr_off.p, sizeof(long long) * (N + 1), cudaMemcpyDeviceToHost));
+    if (csr_ids && c->csr_total) CK(cudaMemcpy(csr_ids, c->csr_ids.p, sizeof(int) * (size_t)c->csr_total, cudaMemcpyDeviceToHost));
+    if (barle_offsets) CK(cudaMemcpy(barle_offsets, c->barle_off.p, sizeof(long long) * (N + 1), cudaMemcpyDeviceToHost));
+    if (barle_bytes && c->barle_total) CK(cudaMemcpy(barle_bytes, c->barle_bytes.p, (size_t)c->barle_total, cudaMemcpyDeviceToHost));
+    if (shadow) CK(cudaMemcpy(shadow, c->shadow.p, sizeof(uint32_t) * N * c->words32, cudaMemcpyDeviceToHost));
+    return SOLAR_GPU_OK;
+}
+
+int solar_gpu_last_timings(solar_gpu_context* c, double* ms, int n)
+{
+    if (!c || !ms) return fail(SOLAR_GPU_ERR_ARG, "NULL argument");
+    if (!c->timed) return 0;
+    CK(cudaEventSynchronize(c->ev[3]));
+    float t[4] = {0, 0, 0, 0};
+    CK(cudaEventElapsedTime(&t[0], c->ev[0], c->ev[1]));
+    CK(cudaEventElapsedTime(&t[1], c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&t[2], c->ev[2], c->ev[3]));
+    CK(cudaEventElapsedTime(&t[3], c->ev[0], c->ev[3]));
+    int k = n < 4 ? n : 4;
+    for (int i = 0; i < k; ++i) ms[i] = t[i];
+    return k;
+}
+
+long long solar_gpu_last_launch_count(solar_gpu_context* c) { return c ? c->launches : -1; }
+
+int solar_gpu_uncompressed_gpu_irradiance(
+    const float* grid_data, int grid_width, int grid_height, int num_total_voxels, int num_top_voxels,
+    const int* pixel_parent, const float* wall_z, float max_height,
+    const float* sun_positions, int num_sun_positions, const float* direct_irradiance, int num_direct,
+    const float* diffuse_irradiance, int num_diffuse, const float* slopes, const float* aspects,
+    float* irradiance_out)
+{
+    return drop_in(SOLAR_GPU_CSR, grid_data, grid_width, grid_height, num_total_voxels, num_top_voxels,
+                   pixel_parent, wall_z, max_height, sun_positions, num_sun_positions, direct_irradiance,
+                   num_direct, diffuse_irradiance, num_diffuse, slopes, aspects, irradiance_out);
+}
+
+int solar_gpu_compressed_gpu_irradiance(
+    const float* grid_data, int grid_width, int grid_height, int num_total_voxels, int num_top_voxels,
+    const int* pixel_parent, const float* wall_z, float max_height,
+    const float* sun_positions, int num_sun_positions, const float* direct_irradiance, int num_direct,
+    const float* diffuse_irradiance, int num_diffuse, const float* slopes, const float* aspects,
+    float* irradiance_out)
+{
+    return drop_in(SOLAR_GPU_BARLE, grid_data, grid_width, grid_height, num_total_voxels, num_top_voxels,
+                   pixel_parent, wall_z, max_height, sun_positions, num_sun_positions, direct_irradiance,
+                   num_direct, diffuse_irradiance, num_diffuse, slopes, aspects, irradiance_out);
+}
+
+}  // extern "C"

@@ -1,0 +1,120 @@
+// Internal types and launchers shared by the translation units of
+// libsolargpu_b200.so.  Nothing here is part of the public C ABI
+// (include/solargpu_b200.h).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sgb {
+
+constexpr int kHoursPerYear = 8760;   // include/pipeline_constants.h:10 of the reference
+constexpr int kMaxDirs = 72 * 36;     // 5 deg x 5 deg bins over both hemispheres
+constexpr int kRawGroup = 16;         // directions buffered per tracer store
+
+// Device error flag bits (set by kernels, read back by the host).
+enum DeviceError : int {
+    kErrBarleStream = 1,   // a ba-RLE stream ran past its byte range or had a bad width code
+    kErrHashFull = 2,      // a dedupe hash probe exceeded its bound
+    kErrListCapacity = 4,  // a neighbor list exceeded the buffer capacity
+};
+
+// One traced direction; host-computed exactly as the reference computes Cdir
+// (include/cuda/viewshed_stage.cuh:64-80), plus the per-direction constants of
+// the DDA (viewshed_kernels.cu:32-40), which are direction-only.
+struct DirEntry {
+    float cx, cy, cz;
+    float ax, ay;      // fmaxf(fabsf(c), 1e-8f)
+    float dX, dY;      // 1.0f / ax, 1.0f / ay (IEEE)
+    int meta;          // bits 0..15: dense sun bin + 1 (0 = none); bit 16: upper hemisphere
+};
+
+// Per daylight hour, FP32 values of the FP64-evaluated solar geometry.
+//   cos_aoi(v) = dot(n_v, s)
+//   direct     = (cos_aoi > 0 && dense >= 0 && !shadow) ? dni_eff * cos_aoi : 0
+//   diffuse    = max(0, c0 * (1 + cos s) + c1 * max(0, cos_aoi) + c2 * sin s)
+struct HourEntry {
+    float sx, sy, sz;
+    float dni_eff;
+    float c0, c1, c2;
+    int dense;         // sun bin (dense index) or -1; padding entries have dense = -1 and zeros
+};
+
+struct DevScene {
+    const float* grid;        // [T]
+    const int* pix_parent;    // [N]
+    const float* wall_z;      // [N - T] or nullptr
+    const float* slopes;      // [N]
+    const float* aspects;     // [N]
+    int W, H, N, T;
+    float maxz;
+};
+
+// Per-voxel geometry derived once per call.
+//   geo_n[v] = (nx, ny, nz, sin slope) with n as in reflection_kernels.cu:59-64
+//   geo_p[v] = (gx, gy, z, 0)
+struct DevGeom {
+    float4* geo_n;
+    float4* geo_p;
+};
+
+// ------------------------------------------------------------------ launchers
+
+// tracer (trace.cu)
+cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
+                         int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
+                         cudaStream_t st);
+cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, cudaStream_t st);
+cudaError_t launch_scan_counts(const int* counts, int n, long long base, long long* offsets,
+                               long long* block_sums, int* block_tmp, cudaStream_t st);
+size_t scan_scratch_elems(int n);
+cudaError_t launch_gather_csr(int chunk_count, int D, const int* raw, const long long* offsets,
+                              int* csr_ids, cudaStream_t st);
+
+// ba-RLE encoder (barle.cu)
+cudaError_t launch_barle_size(int chunk_count, int D, int* raw, const int* counts,
+                              int* sizes, int* err, cudaStream_t st);
+cudaError_t launch_barle_write(int chunk_count, int D, const int* raw, const int* counts,
+                               const long long* offsets, unsigned char* out, int* err,
+                               cudaStream_t st);
+
+// solar (solar.cu)
+cudaError_t launch_hour_table(const float* nudged, const float* dni, const float* dhi,
+                              const int* sun_dense, const int* hour_index, int n_hours,
+                              int n_padded, HourEntry* table, cudaStream_t st);
+cudaError_t launch_voxel_geom(const DevScene& s, DevGeom g, cudaStream_t st);
+cudaError_t launch_solar_slab(const DevGeom& g, int T, const uint32_t* shadow, int words32,
+                              const HourEntry* table, int j0, int B, float* slab, cudaStream_t st);
+cudaError_t launch_solar_hour(const DevGeom& g, int N, const uint32_t* shadow, int words32,
+                              const HourEntry* table, int j, float* hourly, cudaStream_t st);
+cudaError_t launch_solar_sum(const DevGeom& g, int N, const uint32_t* shadow, int words32,
+                             const HourEntry* table, int n_hours, double* sums, cudaStream_t st);
+
+// reflection (reflect.cu)
+struct NeighborLists {
+    int format;                  // 0 = CSR, 1 = ba-RLE
+    const long long* offsets;    // [N + 1] (ids for CSR, bytes for ba-RLE)
+    const int* ids;              // CSR ids, 1-based
+    const unsigned char* bytes;  // ba-RLE stream
+};
+struct Accum {
+    int mode;        // 0 = FP64 sums, 1 = Kahan-compensated FP32, 2 = plain FP32
+    double* f64;     // [N]
+    float* f32;      // [N] (sum) for modes 1, 2
+    float* comp;     // [N] Kahan compensation for mode 1
+};
+cudaError_t launch_reflect_block(const DevGeom& g, int N, int T, const uint32_t* shadow,
+                                 int words32, const HourEntry* table, int j0, int B,
+                                 const float* slab, const NeighborLists& nl, const Accum& acc,
+                                 int* err, cudaStream_t st);
+cudaError_t launch_reflect_hour(const DevGeom& g, int N, int T, const float* hourly,
+                                const NeighborLists& nl, const Accum& acc, int* err,
+                                cudaStream_t st);
+cudaError_t launch_reflect_annual(const DevGeom& g, int N, int T, const double* sums,
+                                  const NeighborLists& nl, double* out, int* err,
+                                  cudaStream_t st);
+cudaError_t launch_finalize(const Accum& acc, int N, float* out, cudaStream_t st);
+cudaError_t launch_finalize_f64(const double* in, int N, float* out, cudaStream_t st);
+
+}  // namespace sgb

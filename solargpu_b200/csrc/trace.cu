@@ -1,0 +1,290 @@
+// Stage 1: hemispherical DDA viewshed over the heightmap.
+//
+// The per-ray arithmetic follows the reference kernel
+// calc_kernel_hemispherical_viewshed_GPU (src/cuda/kernels/viewshed_kernels.cu:7-59)
+// operation for operation, with explicit round-to-nearest intrinsics so the
+// hit cell is bit-identical: the ray height oz + Cdir.z * t is one fused
+// multiply-add, exactly as nvcc contracts it in the reference build.
+//
+// The B200 layout differs from the reference:
+//   * one launch traces all 2592 directions (the reference launches once per
+//     direction and synchronises after each);
+//   * a warp holds 32 consecutive voxels that walk the same direction in
+//     lockstep, so height loads of neighbouring rays share cache lines;
+//   * hits go to a per-voxel raw row [chunk][D] written 16 directions at a
+//     time as 64-byte vectors; the first-occurrence dedupe (the reference's
+//     O(k) global-memory scan per hit, viewshed_kernels.cu:49-55) is a
+//     separate warp-per-voxel pass with a shared-memory hash set and
+//     ballot/popc compaction that keeps direction order;
+//   * shadow bits are packed 32 per word, voxel-major ([N][words32]), and
+//     written once per word.
+#include "sgb_internal.cuh"
+
+namespace sgb {
+namespace {
+
+constexpr int kTraceBlock = 128;
+constexpr int kDedupeWarps = 4;
+constexpr int kHashSlots = 4096;   // > 2592 possible distinct hits per voxel
+
+__device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, int H, float maxz,
+                                         int gx, int gy, float base_z, const DirEntry& d)
+{
+    // Cdir * 2.0f is exact, so these match the reference fused or not.
+    const float ox = __fadd_rn((float)gx, __fmul_rn(d.cx, 2.0f));
+    const float oy = __fadd_rn((float)gy, __fmul_rn(d.cy, 2.0f));
+    const float oz = __fadd_rn(base_z, __fmul_rn(d.cz, 2.0f));
+    int ix = __float2int_rd(ox);
+    int iy = __float2int_rd(oy);
+    const bool px = d.cx >= 0.0f;
+    const bool py = d.cy >= 0.0f;
+    float tMaxX = __fdiv_rn(px ? __fsub_rn(__fadd_rn((float)ix, 1.0f), ox) : __fsub_rn(ox, (float)ix), d.ax);
+    float tMaxY = __fdiv_rn(py ? __fsub_rn(__fadd_rn((float)iy, 1.0f), oy) : __fsub_rn(oy, (float)iy), d.ay);
+    const int sx = px ? 1 : -1;
+    const int sy = py ? 1 : -1;
+    const bool up = (d.meta >> 16) & 1;
+    // Each step moves ix or iy one cell in a fixed direction, so the loop
+    // leaves the grid after at most W + H steps.
+    for (;;) {
+        float t;
+        if (tMaxX < tMaxY) { t = tMaxX; ix += sx; tMaxX = __fadd_rn(tMaxX, d.dX); }
+        else               { t = tMaxY; iy += sy; tMaxY = __fadd_rn(tMaxY, d.dY); }
+        if ((unsigned)ix >= (unsigned)W || (unsigned)iy >= (unsigned)H) return 0;
+        const float zr = __fmaf_rn(d.cz, t, oz);
+        if (up ? (zr > maxz) : (zr < 0.0f)) return 0;
+        const int cell = ix + iy * W;
+        if (__fsub_rn(__ldg(grid + cell), zr) > 0.01f) return cell + 1;
+    }
+}
+
+__global__ void __launch_bounds__(kTraceBlock)
+k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
+        int voxel_offset, int chunk_count, int* __restrict__ raw, uint32_t* __restrict__ shadow)
+{
+    __shared__ int stage[kRawGroup][kTraceBlock];
+    const int lv = blockIdx.x * kTraceBlock + threadIdx.x;
+    const bool active = lv < chunk_count;
+    const int v = voxel_offset + (active ? lv : 0);
+    const int top = __ldg(s.pix_parent + v);
+    const int gx = top % s.W;
+    const int gy = top / s.W;
+    const float base_z = (v < s.T) ? __ldg(s.grid + top) : __ldg(s.wall_z + (v - s.T));
+
+    uint32_t acc = 0;
+    int cur_word = -1;
+    int* row = raw + (size_t)(active ? lv : 0) * D;
+    for (int g0 = 0; g0 < D; g0 += kRawGroup) {
+        for (int k = 0; k < kRawGroup; ++k) {
+            const DirEntry d = dirs[g0 + k];
+            const int hit = active ? trace_ray(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d) : 0;
+            stage[k][threadIdx.x] = hit;
+            const int dense = (d.meta & 0xFFFF) - 1;   // warp-uniform
+            if (dense >= 0) {
+                const int w = dense >> 5;
+                if (w != cur_word) {
+                    if (active && acc) shadow[(size_t)v * words32 + cur_word] = acc;
+                    acc = 0;
+                    cur_word = w;
+                }
+                if (hit) acc |= 1u << (dense & 31);
+            }
+        }
+        if (active) {
+            int4* dst = reinterpret_cast<int4*>(row + g0);
+#pragma unroll
+            for (int q = 0; q < kRawGroup / 4; ++q)
+                dst[q] = make_int4(stage[4 * q][threadIdx.x], stage[4 * q + 1][threadIdx.x],
+                                   stage[4 * q + 2][threadIdx.x], stage[4 * q + 3][threadIdx.x]);
+        }
+    }
+    if (active && acc && cur_word >= 0) shadow[(size_t)v * words32 + cur_word] = acc;
+}
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t x)
+{
+    x *= 0x9E3779B1u;
+    return x >> 20;   // 12 bits
+}
+
+// One warp per voxel: keeps the first occurrence of each hit id in direction
+// order and compacts the row in place; counts[lv] = list length.
+__global__ void __launch_bounds__(kDedupeWarps * 32)
+k_dedupe(int chunk_count, int D, int* __restrict__ raw, int* __restrict__ counts, int* __restrict__ err)
+{
+    extern __shared__ uint32_t tab_all[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    uint32_t* tab = tab_all + warp * kHashSlots;
+    const int lv = blockIdx.x * kDedupeWarps + warp;
+    if (lv >= chunk_count) return;
+    uint4* t4 = reinterpret_cast<uint4*>(tab);
+    for (int i = lane; i < kHashSlots / 4; i += 32) t4[i] = make_uint4(0u, 0u, 0u, 0u);
+    __syncwarp();
+    int* row = raw + (size_t)lv * D;
+    int n = 0;
+    for (int base = 0; base < D; base += 32) {
+        const int d = base + lane;
+        const int h = (d < D) ? row[d] : 0;
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, h);
+        const bool leader = (__ffs(same) - 1) == lane;
+        bool fresh = false;
+        if (h != 0 && leader) {
+            uint32_t slot = hash_slot((uint32_t)h);
+            int probe = 0;
+            for (; probe < kHashSlots; ++probe) {
+                const uint32_t old = atomicCAS(&tab[slot], 0u, (uint32_t)h);
+                if (old == 0u) { fresh = true; break; }
+                if (old == (uint32_t)h) break;
+                slot = (slot + 1) & (kHashSlots - 1);
+            }
+            if (probe == kHashSlots) atomicOr(err, kErrHashFull);
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, fresh);
+        // Writes land below base + 32: every slot there was read this round.
+        if (fresh) row[n + __popc(bal & ((1u << lane) - 1u))] = h;
+        n += __popc(bal);
+    }
+    if (lane == 0) counts[lv] = n;
+}
+
+// ---- exclusive scan of int counts into int64 offsets (3 phases) ----------
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ long long warp_incl_scan(long long x, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Block-wide exclusive scan; returns this thread's exclusive prefix and the block total.
+__device__ long long block_excl_scan(long long x, long long* total)
+{
+    __shared__ long long warp_sums[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long inc = warp_incl_scan(x, lane);
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        long long ws = lane < nw ? warp_sums[lane] : 0;
+        ws = warp_incl_scan(ws, lane);
+        if (lane < nw) warp_sums[lane] = ws;
+    }
+    __syncthreads();
+    const long long before = warp > 0 ? warp_sums[warp - 1] : 0;
+    *total = warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before + inc - x;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_tiles(const int* __restrict__ counts, int n, long long* __restrict__ offsets,
+             long long* __restrict__ tile_sums)
+{
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    long long v[kScanItems];
+    long long local = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        v[i] = (base + i < n) ? counts[base + i] : 0;
+        local += v[i];
+    }
+    long long total;
+    long long run = block_excl_scan(local, &total);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        if (base + i < n) offsets[base + i] = run;
+        run += v[i];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_tile_sums(long long* __restrict__ tile_sums, int ntiles, long long base,
+                 long long* __restrict__ offsets, int n)
+{
+    long long carry = base;
+    for (int i0 = 0; i0 < ntiles; i0 += kScanThreads) {
+        const int i = i0 + threadIdx.x;
+        const long long x = i < ntiles ? tile_sums[i] : 0;
+        long long total;
+        const long long ex = block_excl_scan(x, &total);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) offsets[n] = carry;
+}
+
+__global__ void k_scan_add(long long* __restrict__ offsets, int n, const long long* __restrict__ tile_sums)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) offsets[i] += tile_sums[i / kScanTile];
+}
+
+__global__ void __launch_bounds__(256)
+k_gather_csr(int chunk_count, int D, const int* __restrict__ raw, const long long* __restrict__ offsets,
+             int* __restrict__ csr_ids)
+{
+    const int lv = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (lv >= chunk_count) return;
+    const long long o = offsets[lv];
+    const int k = (int)(offsets[lv + 1] - o);
+    const int* row = raw + (size_t)lv * D;
+    for (int i = lane; i < k; i += 32) csr_ids[o + i] = row[i];
+}
+
+}  // namespace
+
+cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
+                         int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
+                         cudaStream_t st)
+{
+    if (chunk_count <= 0) return cudaSuccess;
+    const int grid = (chunk_count + kTraceBlock - 1) / kTraceBlock;
+    k_trace<<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, cudaStream_t st)
+{
+    if (chunk_count <= 0) return cudaSuccess;
+    const size_t smem = (size_t)kDedupeWarps * kHashSlots * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(k_dedupe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (chunk_count + kDedupeWarps - 1) / kDedupeWarps;
+    k_dedupe<<<grid, kDedupeWarps * 32, smem, st>>>(chunk_count, D, raw, counts, err);
+    return cudaGetLastError();
+}
+
+size_t scan_scratch_elems(int n)
+{
+    return (size_t)((n + kScanTile - 1) / kScanTile) + 1;
+}
+
+cudaError_t launch_scan_counts(const int* counts, int n, long long base, long long* offsets,
+                               long long* block_sums, int* /*unused*/, cudaStream_t st)
+{
+    const int ntiles = (n + kScanTile - 1) / kScanTile;
+    if (n > 0) k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(counts, n, offsets, block_sums);
+    k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(block_sums, ntiles, base, offsets, n);
+    if (n > 0) k_scan_add<<<(n + 255) / 256, 256, 0, st>>>(offsets, n, block_sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_csr(int chunk_count, int D, const int* raw, const long long* offsets,
+                              int* csr_ids, cudaStream_t st)
+{
+    if (chunk_count <= 0) return cudaSuccess;
+    const long long threads = (long long)chunk_count * 32;
+    k_gather_csr<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(chunk_count, D, raw, offsets, csr_ids);
+    return cudaGetLastError();
+}
+
+}  // namespace sgb

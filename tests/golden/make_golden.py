@@ -1,0 +1,134 @@
+"""Generates the golden fixtures under tests/golden/ from the reference's own
+code, compiled from its sources by oracle/Makefile:
+
+  host   (this container, needs the reference tree for oracle/_ref/libref_host.so)
+    scene_<name>.npz      stored input arrays of the small scenes
+    barle_golden.npz      id lists and the reference encoder's bytes
+                          (src/barle_compression.cpp:156-187)
+    sky_<name>.npz        reference sky bins (src/sky_bins.cpp:9-52)
+    voxel_<name>.npz      reference voxelization (src/voxelization.cpp:10-97)
+  gpu    (a CUDA box, needs oracle/_ref/libsolarref.so)
+    ref_stage1_<name>.npz SHA-256 digests + per-voxel sample of the reference
+                          viewshed stage (include/cuda/viewshed_stage.cuh:37-125):
+                          CSR ids, ba-RLE bytes, shadow bitmap
+    ref_annual_<name>.npz the reference API's annual irradiance (both pipelines)
+
+    python tests/golden/make_golden.py host
+    python tests/golden/make_golden.py gpu [--out DIR]
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from solargpu_b200 import inputs  # noqa: E402
+
+SMALL = ("dsm64", "dsm160")
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def save_scene(name: str):
+    s = inputs.make_scene(name)
+    np.savez_compressed(os.path.join(HERE, f"scene_{name}.npz"), width=s.width, height=s.height,
+                        **s.arrays())
+    return s
+
+
+def barle_lists(rng: np.random.Generator) -> list[np.ndarray]:
+    """Id lists covering every width class, long runs (> 255), single-element
+    outliers one class narrower (the optimiser's absorb rule) and empty lists."""
+    out = [np.zeros(0, np.int32), np.array([1], np.int32), np.array([15], np.int32),
+           np.array([16], np.int32), np.array([2 ** 31 - 1], np.int32),
+           np.arange(1, 600, dtype=np.int32), np.arange(1, 2000, 3, dtype=np.int32)]
+    for n in (2, 3, 5, 9, 17, 40, 145, 300, 700, 2592):
+        for scale in (8, 200, 60000, 10_000_000, 2_000_000_000):
+            ids = np.unique(rng.integers(1, scale + 2, size=n)).astype(np.int32)
+            out.append(rng.permutation(ids))
+    for _ in range(60):
+        # mixed gaps: mostly small, some single large jumps
+        gaps = rng.choice([1, 2, 7, 15, 16, 200, 255, 256, 70000, 20_000_000], size=rng.integers(2, 80),
+                          p=[.3, .2, .1, .1, .05, .05, .05, .05, .05, .05])
+        ids = np.cumsum(gaps)
+        ids = ids[ids < 2 ** 31 - 1].astype(np.int32)
+        out.append(rng.permutation(ids))
+    return out
+
+
+def host():
+    if O.ref_host() is None:
+        raise SystemExit("oracle/_ref/libref_host.so is missing (build oracle/ with the reference tree present)")
+    rng = np.random.default_rng(2026)
+    lists = barle_lists(rng)
+    off = np.zeros(len(lists) + 1, np.int64)
+    off[1:] = np.cumsum([len(x) for x in lists])
+    ids = np.concatenate(lists).astype(np.int32)
+    enc = [O.ref_barle_compress(x) for x in lists]
+    boff = np.zeros(len(lists) + 1, np.int64)
+    boff[1:] = np.cumsum([len(b) for b in enc])
+    np.savez_compressed(os.path.join(HERE, "barle_golden.npz"), off=off, ids=ids, boff=boff,
+                        bytes=np.frombuffer(b"".join(enc), np.uint8))
+    for name in SMALL:
+        s = save_scene(name)
+        b = O.ref_sky_bins(s.sun)
+        cfg = inputs.CONFIGS[name]
+        ref_sun = O.ref_sun_positions(cfg.lon, cfg.lat, cfg.tz)
+        np.savez_compressed(os.path.join(HERE, f"sky_{name}.npz"), ref_sun=ref_sun, full_to_dense=b["full_to_dense"],
+                            sun_dense_idx=b["sun_dense_idx"], nudged=b["nudged"],
+                            meta=np.array([b["hsize"], b["vsize"], b["vsize_full"], b["active"], b["words8"]]))
+        H, W = s.height, s.width
+        par, z, asp, sl, ta = O.ref_voxelize(s.grid.reshape(H, W))
+        np.savez_compressed(os.path.join(HERE, f"voxel_{name}.npz"), parent=par, z=z, aspect=asp,
+                            slope=sl, top_aspect=ta)
+    print("host fixtures written to", HERE)
+
+
+def gpu(out_dir: str):
+    if O.ref_gpu() is None:
+        raise SystemExit("oracle/_ref/libsolarref.so is missing")
+    os.makedirs(out_dir, exist_ok=True)
+    for name in SMALL:
+        d = np.load(os.path.join(HERE, f"scene_{name}.npz"))
+        s = inputs.scene_from_arrays(name, d, int(d["width"]), int(d["height"]))
+        r = O.ref_stage1(s)
+        counts = np.diff(r["csr_off"])
+        rng = np.random.default_rng(7)
+        sample = np.sort(rng.choice(s.num_total, size=min(64, s.num_total), replace=False))
+        samp_ids = [r["csr_ids"][r["csr_off"][v]:r["csr_off"][v + 1]] for v in sample]
+        samp_bytes = [r["barle"][r["barle_off"][v]:r["barle_off"][v + 1]] for v in sample]
+        so = np.zeros(len(sample) + 1, np.int64)
+        so[1:] = np.cumsum([len(x) for x in samp_ids])
+        sb = np.zeros(len(sample) + 1, np.int64)
+        sb[1:] = np.cumsum([len(x) for x in samp_bytes])
+        np.savez_compressed(
+            os.path.join(out_dir, f"ref_stage1_{name}.npz"),
+            counts=counts.astype(np.int32), sha_ids=sha(r["csr_ids"].astype(np.int32)),
+            sha_barle=sha(r["barle"]), sha_barle_off=sha(r["barle_off"].astype(np.int64)),
+            sha_svf=sha(r["svf"]), svf_words8=r["svf"].shape[0],
+            sample=sample, sample_off=so, sample_ids=np.concatenate(samp_ids).astype(np.int32),
+            sample_boff=sb, sample_bytes=np.concatenate(samp_bytes).astype(np.uint8),
+            svf=r["svf"] if s.num_total <= 20000 else np.zeros(0, np.uint8))
+        unc = O.ref_irradiance(s, compressed=False)
+        com = O.ref_irradiance(s, compressed=True)
+        np.savez_compressed(os.path.join(out_dir, f"ref_annual_{name}.npz"), uncompressed=unc, compressed=com)
+        print(name, "nnz", int(counts.sum()), "barle bytes", r["barle"].size)
+    print("gpu fixtures written to", out_dir)
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["host", "gpu"])
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    host() if a.what == "host" else gpu(a.out)

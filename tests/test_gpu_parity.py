@@ -1,0 +1,158 @@
+"""GPU parity: the CUDA library (through its C ABI) against the oracle and,
+when it was built, against the reference CUDA pipeline itself.
+
+Integer work (neighbor ids, shadow bits, ba-RLE bytes) must be bit-exact.
+Annual irradiance must be within REL_TOL of the FP64 oracle per voxel."""
+import numpy as np
+import pytest
+
+from conftest import device_arrays, load_scene, oracle_trace
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-4          # max relative error per voxel vs the FP64 oracle
+FLOOR = 1.0             # Wh/m^2 denominator floor (all annual values here are > 1e5)
+
+
+@pytest.fixture(scope="module")
+def ctx(cuda_lib):
+    from solargpu_b200 import api
+    c = api.Context(0)
+    yield c
+    c.close()
+
+
+def fp64_reference(scene):
+    from oracle import oracle as O
+    bins, off, ids, sh = oracle_trace(scene)
+    tot, _ = O.annual_fp64(scene, sh, off, ids)
+    return tot
+
+
+def rel_err(got, want):
+    return np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want), FLOOR)
+
+
+@pytest.mark.parametrize("name", ["dsm64", "dsm160"])
+def test_trace_matches_oracle(ctx, name):
+    from oracle import oracle as O
+    s = load_scene(name)
+    bins, off, ids, sh = oracle_trace(s)
+    r = ctx.trace(s, device_arrays(s))
+    assert r["active_bins"] == bins["active"]
+    np.testing.assert_array_equal(r["csr_off"], off)
+    np.testing.assert_array_equal(r["csr_ids"], ids)
+    np.testing.assert_array_equal(r["shadow"], sh)
+    boff, buf = O.barle_encode_csr(off, ids)
+    np.testing.assert_array_equal(r["barle_off"], boff)
+    np.testing.assert_array_equal(r["barle"], buf)
+
+
+def test_trace_chunked_equals_single(ctx, scene160):
+    dev = device_arrays(scene160)
+    a = ctx.trace(scene160, dev)
+    b = ctx.trace(scene160, dev, chunk_voxels=3001)
+    for k in ("csr_off", "csr_ids", "barle_off", "barle", "shadow"):
+        np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_trace_matches_reference_kernel(ctx, scene64):
+    """Bit-exact against the reference's own viewshed stage rebuilt for sm_100a."""
+    from oracle import oracle as O
+    if O.ref_gpu() is None:
+        pytest.skip("reference CUDA pipeline not built")
+    ref = O.ref_stage1(scene64)
+    r = ctx.trace(scene64, device_arrays(scene64))
+    np.testing.assert_array_equal(r["csr_off"], ref["csr_off"])
+    np.testing.assert_array_equal(r["csr_ids"], ref["csr_ids"])
+    np.testing.assert_array_equal(r["barle_off"], ref["barle_off"])
+    np.testing.assert_array_equal(r["barle"], ref["barle"])
+    np.testing.assert_array_equal(r["shadow"], O.svf_to_words32(ref["svf"], r["shadow_words"]))
+
+
+CASES = [(fmt, B, acc) for fmt in (0, 1) for B in (1, 32, 64, 128, 256) for acc in (0, 1, 2)
+         if not (B == 1 and acc == 1 and fmt == 1)]
+
+
+@pytest.mark.parametrize("fmt,B,acc", CASES)
+def test_irradiance_vs_fp64(ctx, scene64, fmt, B, acc):
+    import torch
+    s = scene64
+    want = fp64_reference(s)
+    out = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
+    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, hour_block=B, accumulation=acc)
+    torch.cuda.synchronize()
+    e = rel_err(out.cpu().numpy(), want)
+    assert e.max() <= REL_TOL, (e.max(), e.mean())
+
+
+@pytest.mark.parametrize("fmt", [0, 1])
+def test_annual_form_vs_fp64(ctx, scene160, fmt):
+    import torch
+    s = scene160
+    want = fp64_reference(s)
+    out = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
+    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, reflection=1)
+    torch.cuda.synchronize()
+    e = rel_err(out.cpu().numpy(), want)
+    assert e.max() <= REL_TOL, (e.max(), e.mean())
+
+
+@pytest.mark.parametrize("fmt", [0, 1])
+def test_hour_block_vs_fp64_dsm160(ctx, scene160, fmt):
+    import torch
+    s = scene160
+    want = fp64_reference(s)
+    out = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
+    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, hour_block=128)
+    torch.cuda.synchronize()
+    e = rel_err(out.cpu().numpy(), want)
+    assert e.max() <= REL_TOL, (e.max(), e.mean())
+
+
+@pytest.mark.parametrize("compressed", [False, True])
+def test_drop_in_entry_points(cuda_lib, scene64, compressed):
+    """The reference-shaped host entry points (host arrays in, host raster out)."""
+    from solargpu_b200 import api
+    s = scene64
+    out = np.zeros(s.num_total, np.float32)
+    fn = api.compressed_gpu_irradiance if compressed else api.uncompressed_gpu_irradiance
+    rc = fn(s.grid, s.width, s.height, s.num_total, s.num_top, s.pixel_parent, s.wall_z, s.max_height,
+            s.sun, s.direct, s.diffuse, s.slopes, s.aspects, out)
+    assert rc == 0
+    e = rel_err(out, fp64_reference(s))
+    assert e.max() <= REL_TOL, (e.max(), e.mean())
+
+
+@pytest.mark.parametrize("compressed", [False, True])
+def test_drop_in_vs_reference_api(cuda_lib, scene64, compressed):
+    """Against the reference API rebuilt for sm_100a (FP32 per-hour sums):
+    both sit near the FP64 oracle; ours is the closer one."""
+    from oracle import oracle as O
+    from solargpu_b200 import api
+    if O.ref_gpu() is None:
+        pytest.skip("reference CUDA pipeline not built")
+    s = scene64
+    ref = O.ref_irradiance(s, compressed)
+    out = np.zeros(s.num_total, np.float32)
+    fn = api.compressed_gpu_irradiance if compressed else api.uncompressed_gpu_irradiance
+    fn(s.grid, s.width, s.height, s.num_total, s.num_top, s.pixel_parent, s.wall_z, s.max_height,
+       s.sun, s.direct, s.diffuse, s.slopes, s.aspects, out)
+    want = fp64_reference(s)
+    e_ours, e_ref = rel_err(out, want), rel_err(ref, want)
+    assert e_ours.max() <= REL_TOL
+    assert rel_err(out, ref.astype(np.float64)).max() <= max(2 * REL_TOL, 2 * e_ref.max())
+    assert e_ours.mean() <= e_ref.mean() * 1.01 + 1e-9
+
+
+def test_invalid_pixel_parent_is_rejected(ctx, scene64):
+    import torch
+    from solargpu_b200 import api
+    dev = device_arrays(scene64)
+    dev["pixel_parent"] = dev["pixel_parent"].clone()
+    dev["pixel_parent"][scene64.num_top + 3] = scene64.num_top + 5   # wall parent out of range
+    out = torch.zeros(scene64.num_total, dtype=torch.float32, device="cuda:0")
+    with pytest.raises(api.SolarGPUError) as e:
+        ctx.run_device(scene64, dev, out)
+    assert e.value.code == -1
+    ctx.run_device(scene64, device_arrays(scene64), out)   # the context stays usable

@@ -1,0 +1,139 @@
+"""CPU checks of the oracle and of the caller-side inputs against the
+reference's own code (golden fixtures made by tests/golden/make_golden.py)."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_scene, oracle_trace
+
+
+def _lists(d, off_key="off", ids_key="ids"):
+    off, ids = d[off_key], d[ids_key]
+    return [ids[off[i]:off[i + 1]] for i in range(off.size - 1)]
+
+
+def test_barle_encoder_matches_reference(oracle_lib):
+    """Byte-exact to src/barle_compression.cpp:156-187 on lists covering every
+    width class, runs longer than 255, the absorb rule, and empty lists."""
+    d = np.load(os.path.join(GOLDEN, "barle_golden.npz"))
+    lists = _lists(d)
+    ref = [d["bytes"][d["boff"][i]:d["boff"][i + 1]].tobytes() for i in range(len(lists))]
+    for ids, want in zip(lists, ref):
+        assert oracle_lib.barle_encode(ids) == want
+
+
+def test_barle_roundtrip(oracle_lib):
+    d = np.load(os.path.join(GOLDEN, "barle_golden.npz"))
+    for ids in _lists(d):
+        dec = oracle_lib.barle_decode(oracle_lib.barle_encode(ids))
+        want = np.unique(ids.astype(np.uint32))[::-1]
+        assert np.array_equal(dec, want)
+
+
+def test_barle_csr_encoder_concatenates(oracle_lib):
+    d = np.load(os.path.join(GOLDEN, "barle_golden.npz"))
+    boff, buf = oracle_lib.barle_encode_csr(d["off"], d["ids"])
+    assert np.array_equal(boff, d["boff"])
+    assert np.array_equal(buf, d["bytes"])
+
+
+@pytest.mark.parametrize("cut", [1, 2, 3, 4])
+def test_barle_decoder_rejects_truncated(oracle_lib, cut):
+    enc = oracle_lib.barle_encode(np.arange(1, 300, 7, dtype=np.int32))
+    with pytest.raises(ValueError):
+        oracle_lib.barle_decode(enc[:-cut] if cut < 4 else enc[:2])
+
+
+def test_barle_decoder_rejects_bad_code(oracle_lib):
+    enc = bytearray(oracle_lib.barle_encode(np.array([5, 3, 1], np.int32)))
+    enc[0] = (enc[0] & 0x1F) | (5 << 5)   # first 3-bit code -> 5 (unused)
+    with pytest.raises(ValueError):
+        oracle_lib.barle_decode(bytes(enc))
+
+
+@pytest.mark.parametrize("name", ["dsm64", "dsm160"])
+def test_sky_bins_match_reference(oracle_lib, name):
+    s = load_scene(name)
+    g = np.load(os.path.join(GOLDEN, f"sky_{name}.npz"))
+    b = oracle_lib.sky_bins(s.sun)
+    assert np.array_equal(b["full_to_dense"], g["full_to_dense"])
+    assert np.array_equal(b["sun_dense_idx"], g["sun_dense_idx"])
+    assert np.array_equal(b["nudged"], g["nudged"])
+    assert [b["hsize"], b["vsize"], b["vsize_full"], b["active"], b["words8"]] == list(g["meta"])
+
+
+def test_sun_positions_match_reference():
+    from solargpu_b200 import inputs
+    g = np.load(os.path.join(GOLDEN, "sky_dsm64.npz"))
+    c = inputs.CONFIGS["dsm64"]
+    assert np.array_equal(inputs.sun_positions(c.lon, c.lat, c.tz), g["ref_sun"][:8760])
+
+
+@pytest.mark.parametrize("name", ["dsm64", "dsm160"])
+def test_voxelization_matches_reference(name):
+    """The caller-side voxelization agrees with src/voxelization.cpp:10-97
+    (parents and heights exactly; angles to float rounding)."""
+    from solargpu_b200 import inputs
+    s = load_scene(name)
+    g = np.load(os.path.join(GOLDEN, f"voxel_{name}.npz"))
+    par, z, asp = inputs.detect_wall_voxels(s.grid.reshape(s.height, s.width))
+    assert np.array_equal(par, g["parent"])
+    assert np.array_equal(z, g["z"])
+    assert np.allclose(asp, g["aspect"], rtol=0, atol=2e-6)
+    sl, ta = inputs.top_slope_aspect(s.grid.reshape(s.height, s.width))
+    assert np.allclose(sl, g["slope"], rtol=0, atol=2e-6)
+    assert np.allclose(ta, g["top_aspect"], rtol=0, atol=2e-6)
+
+
+def test_scene_generator_is_deterministic():
+    from solargpu_b200 import inputs
+    a = inputs.make_scene("dsm64")
+    b = load_scene("dsm64")
+    for k, v in a.arrays().items():
+        assert np.array_equal(v, b.arrays()[k]), k
+
+
+def test_trace_lists_are_first_occurrence_unique(scene64):
+    bins, off, ids, sh = oracle_trace(scene64)
+    assert off[0] == 0 and off[-1] == ids.size
+    assert ids.min() >= 1 and ids.max() <= scene64.num_top
+    for v in range(0, scene64.num_total, 97):
+        l = ids[off[v]:off[v + 1]]
+        assert np.unique(l).size == l.size
+    assert sh.shape == (scene64.num_total, (bins["active"] + 31) // 32)
+
+
+@pytest.mark.parametrize("name", ["dsm64", "dsm160"])
+def test_oracle_trace_matches_reference_gpu_golden(name):
+    """Oracle DDA vs the reference CUDA kernel's own output (digests of the
+    full CSR ids, ba-RLE stream and shadow bitmap, made on a B200)."""
+    path = os.path.join(GOLDEN, f"ref_stage1_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip("reference GPU fixture not generated yet")
+    from oracle import oracle as O
+    g = np.load(path)
+    s = load_scene(name)
+    bins, off, ids, sh = oracle_trace(s)
+    assert np.array_equal(np.diff(off).astype(np.int32), g["counts"])
+    assert hashlib.sha256(ids.astype(np.int32).tobytes()).hexdigest() == str(g["sha_ids"])
+    boff, buf = O.barle_encode_csr(off, ids)
+    assert hashlib.sha256(buf.tobytes()).hexdigest() == str(g["sha_barle"])
+    svf8 = np.zeros((int(g["svf_words8"]), s.num_total), np.uint8)
+    bytes_ = sh.view(np.uint8).reshape(s.num_total, -1)[:, :int(g["svf_words8"])]
+    svf8[:] = bytes_.T
+    assert hashlib.sha256(svf8.tobytes()).hexdigest() == str(g["sha_svf"])
+
+
+def test_fp64_forms_agree(scene64):
+    """Annual-sum form and per-hour form of the FP64 oracle (linearity)."""
+    from oracle import oracle as O
+    bins, off, ids, sh = oracle_trace(scene64)
+    tot, dd = O.annual_fp64(scene64, sh, off, ids)
+    v0, v1 = 100, 400
+    hr = O.hourly_fp64(scene64, sh, off, ids, v0, v1, hblock=97)
+    assert np.allclose(hr, tot[v0:v1], rtol=1e-12, atol=0)
+    v0, v1 = scene64.num_top + 10, scene64.num_top + 200
+    hr = O.hourly_fp64(scene64, sh, off, ids, v0, v1, hblock=64)
+    assert np.allclose(hr, tot[v0:v1], rtol=1e-12, atol=0)
