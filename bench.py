@@ -1,0 +1,417 @@
+"""Benchmark: annual voxel-hours/s of the whole irradiance path on B200.
+
+One step = one complete annual run on the resident scene: Stage 1 (DDA
+viewshed tracer, neighbor lists, shadow bits) and Stage 2/3 (solar +
+hour-block reflection + accumulation over all daylight hours).
+voxel-hours = voxels x daylight hours.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica of the workload (the
+path shards by DSM tile with no exchange), value = all ranks' voxel-hours /
+the slowest rank's time.  `--impl reference` times the reference's own
+implementation (its CUDA pipeline rebuilt from source for sm_100a, called
+through its stock API) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "annual voxel-hours/s on 1 B200 vs plain per-hour path at ≤1e-4 rel err"
+UNIT = "voxel-hours/s"
+FMT_NAMES = {0: "CSR", 1: "ba-RLE"}
+ACC_NAMES = {0: "fp32 block sums + fp64 annual", 1: "kahan-compensated fp32", 2: "plain fp32"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="dsm1024")
+    ap.add_argument("--format", type=int, default=1, help="0 = CSR, 1 = ba-RLE")
+    ap.add_argument("--hour-block", type=int, default=256)
+    ap.add_argument("--accumulation", type=int, default=1)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-hour comparison run")
+    ap.add_argument("--no-check", action="store_true", help="skip the FP64 error check")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x: float, device) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+_PINNED = []
+
+
+def pinned_copy(a: np.ndarray) -> np.ndarray:
+    """A copy of `a` in page-locked host memory (kept alive for the run)."""
+    import torch
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    _PINNED.append(t)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
+def workload_desc(scene, name: str) -> str:
+    from solargpu_b200 import inputs
+    c = inputs.CONFIGS[name]
+    return (f"{name}: seeded synthetic DSM {c.size}x{c.size} @1 m, {c.n_buildings} buildings "
+            f"({c.side_min}-{c.side_max} m, roofs {c.roof_min:g}-{c.roof_max:g} m), {c.n_trees} Gaussian trees, "
+            f"{scene.num_top} top + {scene.num_total - scene.num_top} wall voxels, "
+            f"lat {c.lat} lon {c.lon} tz +{c.tz}, synthetic TMY")
+
+
+def roofline_bytes(scene, ctx_sizes, fmt, B, acc) -> float:
+    """Algorithmic HBM bytes of one hour-block reflection launch (gathered slab
+    rows counted once, as cache hits): neighbor stream + offsets + geometry +
+    shadow words + accumulator read/write per voxel, plus one read of the
+    block's top-cell slab."""
+    csr_entries, barle_bytes, words32 = ctx_sizes
+    N, T = scene.num_total, scene.num_top
+    lists = barle_bytes if fmt == 1 else 4 * csr_entries
+    acc_b = 16 if acc in (0, 1) else 8
+    return float(lists + N * (8 + 32 + 4 * words32 + acc_b) + T * B * 4)
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    from solargpu_b200 import api, inputs
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scene = inputs.make_scene(args.workload)
+    N, T = scene.num_total, scene.num_top
+    d = {
+        "grid": torch.from_numpy(scene.grid).to(dev),
+        "pixel_parent": torch.from_numpy(scene.pixel_parent).to(dev),
+        "wall_z": torch.from_numpy(scene.wall_z).to(dev),
+        "slopes": torch.from_numpy(scene.slopes).to(dev),
+        "aspects": torch.from_numpy(scene.aspects).to(dev),
+    }
+    out = torch.empty(N, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+    ctx = api.Context(local)
+    opts = dict(neighbor_format=args.format, hour_block=args.hour_block, accumulation=args.accumulation,
+                use_graph=0, time_kernels=1)
+
+    def step():
+        ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    # ---- timed region
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(pg)
+    torch.cuda.synchronize(dev)
+    evs = []
+    ktimes = {}
+    launches = 0
+    for _ in range(args.steps):
+        flush.zero_()                       # untimed L2 flush between steps
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        evs.append((e0, e1))
+        for g, (ms, n) in ctx.kernel_times().items():
+            a = ktimes.setdefault(g, [0.0, 0])
+            a[0] += ms
+            a[1] += n
+        launches += ctx.launches()
+    torch.cuda.synchronize(dev)
+    barrier(pg)
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(pg, sum(step_ms), dev)
+    import ctypes as C
+    ne, nb = C.c_longlong(), C.c_longlong()
+    w, a_, n_ = C.c_int(), C.c_int(), C.c_int()
+    api.lib().solar_gpu_trace_sizes(ctx.h, C.byref(ne), C.byref(nb), C.byref(w), C.byref(a_), C.byref(n_))
+    Hd = int(((scene.sun[:, 1] - np.float32(1e-8)) >= 1.0).sum())
+    units = float(N) * Hd
+    value = world * units * args.steps / (total_ms / 1e3)
+    ms_per_step = total_ms / args.steps
+
+    # ---- dominant kernel roofline (live events over the timed region)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom = max(ktimes.items(), key=lambda kv: kv[1][0])
+    refl_ms, refl_n = ktimes.get("reflect", (0.0, 0))
+    B = args.hour_block
+    alg = roofline_bytes(scene, (ne.value, nb.value, w.value), args.format, B, args.accumulation)
+    per_launch_ms = refl_ms / max(1, refl_n)
+    achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"reflect_block_{args.workload}_{FMT_NAMES[args.format].replace('-', '').lower()}_b{B}.md")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.strip().startswith("traffic_bytes_per_launch:"):
+                try:
+                    traffic = float(ln.split(":", 1)[1].split()[0])
+                except ValueError:
+                    pass
+    roof = {"bound": "hbm", "kernel": "k_reflect_block (hour-block SpMM + accumulation)",
+            "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(achieved / hbm_peak, 5), "peak_source": peak_src,
+            "traffic": traffic, "alg_bytes_per_launch": alg, "launch_ms": round(per_launch_ms, 4),
+            "share_of_step": round(refl_ms / max(1e-9, sum(v[0] for v in ktimes.values())), 4),
+            "dominant_group": dom[0]}
+
+    # ---- end to end through the host API (pinned host buffers in and out)
+    e2e = None
+    if True:
+        hs = inputs.Scene(scene.name, pinned_copy(scene.grid), scene.width, scene.height, N, T,
+                          pinned_copy(scene.pixel_parent), pinned_copy(scene.wall_z), scene.max_height,
+                          pinned_copy(scene.sun), pinned_copy(scene.direct), pinned_copy(scene.diffuse),
+                          pinned_copy(scene.slopes), pinned_copy(scene.aspects))
+        hout = pinned_copy(np.zeros(N, np.float32))
+        eopts = dict(neighbor_format=args.format, hour_block=B, accumulation=args.accumulation, use_graph=1)
+        ctx.run_host(hs, hout, **eopts)
+        barrier(pg)
+        wall = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            ctx.run_host(hs, hout, **eopts)
+            wall.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks(pg, sum(wall), dev)
+        h2d = 4 * (T + N + (N - T) + 2 * N) + 4 * 8760 * 4
+        e2e = {"value": world * units * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 4 * N, "api": "solar_gpu_run_host (C ABI, host buffers)"}
+
+    extra = {}
+    if rank == 0 and not args.no_plain:
+        # plain per-hour path on the same GPU (the metric's comparison)
+        popts = dict(neighbor_format=args.format, hour_block=1, accumulation=2, use_graph=0, time_kernels=0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        e0.record(stream)
+        ctx.run_device(scene, d, out, stream=stream.cuda_stream, **popts)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_ms = e0.elapsed_time(e1)
+        extra["plain_per_hour"] = {"ms_per_step": round(plain_ms, 2), "value": units / (plain_ms / 1e3),
+                                   "speedup": round(plain_ms / ms_per_step, 2),
+                                   "config": "hour_block 1 (one solar + one reflection launch per daylight hour), plain fp32"}
+        ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
+        torch.cuda.synchronize(dev)
+    if rank == 0 and not args.no_check:
+        from oracle import oracle as O
+        r = ctx.trace(scene, d, neighbor_format=0)
+        ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
+        torch.cuda.synchronize(dev)
+        tot, _ = O.annual_fp64(scene, r["shadow"], r["csr_off"], r["csr_ids"])
+        got = out.cpu().numpy().astype(np.float64)
+        rel = np.abs(got - tot) / np.maximum(np.abs(tot), 1.0)
+        extra["error_vs_fp64"] = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),
+                                  "oracle": "FP64 annual-sum form on the GPU-built neighbor lists and shadow bits"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        rng = np.random.default_rng(0)
+        ns = min(N, 20000)
+        smp = np.sort(rng.choice(N, ns, replace=False))
+        r = O.cpu_sample(scene, smp, hblock=128)
+        cpu = {"value": r["voxel_hours_per_s"], "unit": UNIT, "cores": r["threads"], "kind": "port",
+               "sample": (f"FP64 oracle, per-hour method: full trace of {ns} random voxels ({r['trace_s']:.2f} s), "
+                          f"top-cell solar table for one {r['hblock']}-hour block ({r['table_s']:.2f} s), "
+                          f"per-hour reflection sums of the {ns} voxels for that block ({r['sums_s']:.2f} s); "
+                          f"scaled to {N} voxels x {r['hours']} h")}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_desc(scene, args.workload), "voxels": N, "daylight_hours": Hd,
+                       "neighbor_format": FMT_NAMES[args.format], "hour_block": B,
+                       "accumulation": ACC_NAMES[args.accumulation],
+                       "l2": "256 MiB buffer written between timed steps (outside the events)",
+                       "parallelism": f"{world} independent replica(s), no exchange"},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "stage_ms": {g: round(v[0] / args.steps, 3) for g, v in ktimes.items()},
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+# ---------------------------------------------------------------- reference arm
+
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null (the reference prints progress from C++)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def run_reference(args, world, rank, local, pg):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from solargpu_b200 import inputs
+    if O.ref_gpu() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsolarref.so was not built"}))
+        return
+    scene = inputs.make_scene(args.workload)
+    comp = args.format == 1
+    Hd = int(((scene.sun[:, 1] - np.float32(1e-8)) >= 1.0).sum())
+    units = float(scene.num_total) * Hd
+    for _ in range(args.warmup):
+        with quiet_stdout():
+            O.ref_irradiance(scene, comp)
+    wall = []
+    for _ in range(args.steps):
+        with quiet_stdout():
+            t0 = time.perf_counter()
+            O.ref_irradiance(scene, comp)   # synchronous stock API (H2D, both stages, D2H)
+            wall.append(time.perf_counter() - t0)
+    sec = sum(wall)
+    value = units * args.steps / sec
+    desc = ("reference CUDA pipeline (src/cuda/*.cu, sm_100a build of the unmodified sources) through its stock "
+            f"API solar_gpu::{'compressed' if comp else 'uncompressed'}_gpu_irradiance, host buffers in/out; "
+            "one full annual run per step")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": workload_desc(scene, args.workload), "voxels": scene.num_total,
+                       "daylight_hours": Hd, "neighbor_format": FMT_NAMES[args.format]},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": desc + " (the reference has no CPU path; its host thread drives the GPU)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, local, pg)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

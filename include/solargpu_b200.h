@@ -54,6 +54,12 @@ typedef struct solar_gpu_options {
                                 SOLAR_GPU_REFL_ANNUAL (sum over hours first, one sparse product) */
     long long chunk_voxels;  /* tracer chunk in voxels (bounds the raw hit buffer); 0 = from free memory */
     int use_graph;           /* capture the hour-block loop in a CUDA graph */
+    int time_kernels;        /* record CUDA events around every kernel group (no graph); see
+                                solar_gpu_kernel_times */
+    int group_size;          /* hour-block reflection kernel: 0 = one warp per voxel, list decoded
+                                in every block; 4 or 8 = voxels sharing one warp, their lists
+                                merged once per run into weighted union entries (hour_block <= 128
+                                for 8, <= 256 for 4) */
 } solar_gpu_options;
 
 void solar_gpu_default_options(solar_gpu_options* opt);
@@ -147,6 +153,22 @@ int solar_gpu_trace_copy(solar_gpu_context* ctx, long long* csr_offsets, int* cs
    [2] Stage 2/3 (solar + reflection + accumulation), [3] total.
    Returns the number of values written. */
 int solar_gpu_last_timings(solar_gpu_context* ctx, double* ms, int n);
+
+/* Per kernel group device time of the last run with time_kernels set:
+   ms[i] and launches[i] for i < SOLAR_GPU_KT_COUNT.  Returns the count. */
+enum {
+    SOLAR_GPU_KT_SETUP = 0,      /* hour table, voxel geometry, input check */
+    SOLAR_GPU_KT_TRACE = 1,      /* DDA tracer */
+    SOLAR_GPU_KT_DEDUPE = 2,     /* first-occurrence dedupe */
+    SOLAR_GPU_KT_CSR = 3,        /* offsets scan + CSR gather */
+    SOLAR_GPU_KT_BARLE = 4,      /* ba-RLE size, scan, write */
+    SOLAR_GPU_KT_SOLAR = 5,      /* solar slab / hourly / annual-sum kernels */
+    SOLAR_GPU_KT_REFLECT = 6,    /* reflection + accumulation kernels */
+    SOLAR_GPU_KT_FINALIZE = 7,
+    SOLAR_GPU_KT_GROUP = 8,      /* grouped-reflection build (once per run) */
+    SOLAR_GPU_KT_COUNT = 9
+};
+int solar_gpu_kernel_times(solar_gpu_context* ctx, double* ms, long long* launches, int n);
 
 /* Number of kernel launches the library issued in the last run. */
 long long solar_gpu_last_launch_count(solar_gpu_context* ctx);

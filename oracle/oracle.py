@@ -300,3 +300,25 @@ def svf_to_words32(svf8: np.ndarray, words32: int) -> np.ndarray:
     pad[:w8] = svf8
     b = pad.T.reshape(n, words32, 4).astype(np.uint32)
     return (b[..., 0] | (b[..., 1] << 8) | (b[..., 2] << 16) | (b[..., 3] << 24)).astype(np.uint32)
+
+
+def cpu_sample(scene, sample: np.ndarray, hblock: int = 64, nthreads: int | None = None) -> dict:
+    """Times the FP64 per-hour method on a bounded sample (see orc_cpu_sample)
+    and scales it to the whole scene.  Returns seconds per stage and the
+    estimated whole-scene voxel-hours/s."""
+    sample = np.ascontiguousarray(sample, np.int32)
+    times = np.zeros(3, np.float64)
+    wall = scene.wall_z if scene.wall_z.size else np.zeros(1, np.float32)
+    nthreads = nthreads or os.cpu_count() or 1
+    nh = lib().orc_cpu_sample(_ptr(scene.grid), scene.width, scene.height, scene.num_total, scene.num_top,
+                              _ptr(scene.pixel_parent), _ptr(wall), C.c_float(scene.max_height),
+                              _ptr(scene.slopes), _ptr(scene.aspects), _ptr(np.ascontiguousarray(scene.sun, np.float32)),
+                              _ptr(scene.direct), _ptr(scene.diffuse), _ptr(sample), sample.size, hblock, nthreads,
+                              _ptr(times))
+    ns = sample.size
+    hb = min(hblock, nh)
+    blocks = nh / hb
+    t_full = times[0] / ns * scene.num_total + (times[1] + times[2] / ns * scene.num_total) * blocks
+    return dict(trace_s=float(times[0]), table_s=float(times[1]), sums_s=float(times[2]), hours=int(nh),
+                hblock=int(hb), threads=int(nthreads), est_full_s=float(t_full),
+                voxel_hours_per_s=float(scene.num_total * nh / t_full))

@@ -809,3 +809,202 @@ int orc_hour_table_dump(const float* sun_az_alt, const float* dni, const float* 
     free(sdi); free(nudged); free(hours);
     return nh;
 }
+
+/* ------------------------------------------------------------------ */
+/* CPU baseline sample: times the FP64 method on a bounded sample of a   */
+/* scene.  Stage 1 = full 2592-direction trace + dedupe of `ns` sampled  */
+/* voxels; Stage 2/3 = one block of `hblock` daylight hours: the top-cell */
+/* solar table for all T cells, then the per-hour reflection sums of the */
+/* sampled voxels.  Returns wall seconds in times[0..2] = {trace, table, */
+/* voxel sums}; the caller scales them to the whole workload.            */
+/* ------------------------------------------------------------------ */
+
+#include <time.h>
+
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+typedef struct {
+    const orc_scene* s;
+    const int* sample; int a, b;
+    int* nb; int* cnt; uint32_t* sh; int words32;
+} sample_job;
+
+static void* sample_trace_worker(void* arg)
+{
+    sample_job* j = (sample_job*)arg;
+    const orc_scene* s = j->s;
+    orc_set st;
+    st.key = (int*)malloc(4096 * sizeof(int));
+    st.gen = (int*)calloc(4096, sizeof(int));
+    st.cur = 0;
+    for (int i = j->a; i < j->b; ++i) {
+        int v = j->sample[i];
+        int* out = j->nb + (size_t)i * s->D;
+        uint32_t* sh = j->sh + (size_t)i * j->words32;
+        memset(sh, 0, sizeof(uint32_t) * (size_t)j->words32);
+        ++st.cur;
+        int n = 0;
+        for (int d = 0; d < s->D; ++d) {
+            int hit = trace_ray(s, v, s->dirs[3 * d], s->dirs[3 * d + 1], s->dirs[3 * d + 2], s->upper[d]);
+            if (!hit) continue;
+            if (s->dense[d] >= 0) sh[s->dense[d] >> 5] |= 1u << (s->dense[d] & 31);
+            if (set_insert(&st, hit)) out[n++] = hit;
+        }
+        j->cnt[i] = n;
+    }
+    free(st.key); free(st.gen);
+    return NULL;
+}
+
+typedef struct {
+    const orc_scene* s; const float *slopes, *aspects;
+    const orc_hour* hours; int h0, h1;
+    double* Itop; int a, b;
+    const int* sample; const int* nb; const int* cnt; const uint32_t* sh; int words32;
+    double* out;
+} sample_irr_job;
+
+static void* sample_table_worker(void* arg)
+{
+    sample_irr_job* j = (sample_irr_job*)arg;
+    int hb = j->h1 - j->h0;
+    for (int g = j->a; g < j->b; ++g) {
+        orc_vox gv;
+        vox_geom(j->s, j->slopes, j->aspects, g, &gv);
+        for (int h = j->h0; h < j->h1; ++h)
+            j->Itop[(size_t)g * hb + (h - j->h0)] = solar_I(&gv, &j->hours[h], 0);
+    }
+    return NULL;
+}
+
+static void* sample_sum_worker(void* arg)
+{
+    sample_irr_job* j = (sample_irr_job*)arg;
+    int hb = j->h1 - j->h0;
+    double* acc = (double*)malloc(sizeof(double) * (size_t)hb);
+    for (int i = j->a; i < j->b; ++i) {
+        int v = j->sample[i];
+        orc_vox me;
+        vox_geom(j->s, j->slopes, j->aspects, v, &me);
+        for (int h = 0; h < hb; ++h)
+            acc[h] = solar_I(&me, &j->hours[j->h0 + h], bit_of(j->sh, j->words32, i, j->hours[j->h0 + h].dense));
+        const int* l = j->nb + (size_t)i * j->s->D;
+        for (int k = 0; k < j->cnt[i]; ++k) {
+            double w = refl_w(j->s, &me, l[k] - 1);
+            if (w == 0.0) continue;
+            const double* row = j->Itop + (size_t)(l[k] - 1) * hb;
+            for (int h = 0; h < hb; ++h) acc[h] += w * row[h];
+        }
+        double sum = 0.0;
+        for (int h = 0; h < hb; ++h) sum += acc[h];
+        j->out[i] = sum;
+    }
+    free(acc);
+    return NULL;
+}
+
+int orc_cpu_sample(const float* grid, int W, int H, int num_total, int num_top,
+                   const int* pix_parent, const float* wall_z, float maxz,
+                   const float* slopes, const float* aspects,
+                   const float* sun_az_alt, const float* dni, const float* dhi,
+                   const int* sample, int ns, int hblock, int nthreads, double* times)
+{
+    int fd[72 * 18 + 64], meta[5];
+    int* sdi = (int*)malloc(sizeof(int) * ORC_HOURS);
+    float* nudged = (float*)malloc(sizeof(float) * 2 * ORC_HOURS);
+    orc_hour* hours = (orc_hour*)malloc(sizeof(orc_hour) * ORC_HOURS);
+    orc_sky_bins(sun_az_alt, 5.0f, 5.0f, fd, sdi, nudged, meta);
+    int nh = orc_hour_table(nudged, sdi, dni, dhi, hours);
+    int D = meta[0] * meta[2];
+    float* dirs = (float*)malloc(sizeof(float) * 3 * D);
+    int* dense = (int*)malloc(sizeof(int) * D);
+    int* upper = (int*)malloc(sizeof(int) * D);
+    orc_directions(meta[0], meta[1], 5.0f, 5.0f, fd, dirs, dense, upper);
+    int words32 = (meta[3] + 31) / 32;
+    if (words32 < 1) words32 = 1;
+    orc_scene s = { grid, W, H, num_total, num_top, pix_parent, wall_z, maxz, dirs, dense, upper, D, 1 };
+    if (nthreads < 1) nthreads = 1;
+    if (hblock > nh) hblock = nh;
+    int* nb = (int*)malloc(sizeof(int) * (size_t)ns * D);
+    int* cnt = (int*)malloc(sizeof(int) * (size_t)ns);
+    uint32_t* sh = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)ns * words32);
+    double* Itop = (double*)malloc(sizeof(double) * (size_t)num_top * (size_t)hblock);
+    double* out = (double*)malloc(sizeof(double) * (size_t)ns);
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+    sample_job* tj = (sample_job*)calloc((size_t)nthreads, sizeof(sample_job));
+    sample_irr_job* ij = (sample_irr_job*)calloc((size_t)nthreads, sizeof(sample_irr_job));
+
+    double t0 = now_s();
+    for (int t = 0; t < nthreads; ++t) {
+        tj[t].s = &s; tj[t].sample = sample;
+        tj[t].a = (int)((long long)ns * t / nthreads); tj[t].b = (int)((long long)ns * (t + 1) / nthreads);
+        tj[t].nb = nb; tj[t].cnt = cnt; tj[t].sh = sh; tj[t].words32 = words32;
+        pthread_create(&th[t], NULL, sample_trace_worker, &tj[t]);
+    }
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+    double t1 = now_s();
+    for (int pass = 0; pass < 2; ++pass) {
+        int n = pass == 0 ? num_top : ns;
+        for (int t = 0; t < nthreads; ++t) {
+            sample_irr_job* j = &ij[t];
+            j->s = &s; j->slopes = slopes; j->aspects = aspects; j->hours = hours;
+            j->h0 = 0; j->h1 = hblock; j->Itop = Itop;
+            j->a = (int)((long long)n * t / nthreads); j->b = (int)((long long)n * (t + 1) / nthreads);
+            j->sample = sample; j->nb = nb; j->cnt = cnt; j->sh = sh; j->words32 = words32; j->out = out;
+            pthread_create(&th[t], NULL, pass == 0 ? sample_table_worker : sample_sum_worker, j);
+        }
+        for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+        if (pass == 0) times[1] = now_s() - t1;
+    }
+    times[0] = t1 - t0;
+    times[2] = now_s() - t1 - times[1];
+    free(th); free(tj); free(ij); free(nb); free(cnt); free(sh); free(Itop); free(out);
+    free(dirs); free(dense); free(upper); free(sdi); free(nudged); free(hours);
+    return nh;
+}
+
+/* Step counts of every (voxel, direction) ray, for studying lane grouping of
+   the GPU tracer.  steps: [(v1-v0)][D] (int16, saturating). */
+static int trace_ray_steps(const orc_scene* s, int t_id, float cx, float cy, float cz, int is_upper)
+{
+    int top_id = s->pix_parent[t_id];
+    int gx = top_id % s->W, gy = top_id / s->W;
+    float base_z = (t_id < s->num_top) ? s->grid[gx + gy * s->W] : s->wall_z[t_id - s->num_top];
+    float ox = (float)gx + cx * 2.0f, oy = (float)gy + cy * 2.0f, oz = base_z + cz * 2.0f;
+    int ix = (int)floorf(ox), iy = (int)floorf(oy);
+    float ax = fmaxf(fabsf(cx), 1e-8f), ay = fmaxf(fabsf(cy), 1e-8f);
+    float tMaxX = ((cx >= 0.0f) ? ((float)ix + 1.0f - ox) : (ox - (float)ix)) / ax;
+    float tMaxY = ((cy >= 0.0f) ? ((float)iy + 1.0f - oy) : (oy - (float)iy)) / ay;
+    float dX = 1.0f / ax, dY = 1.0f / ay;
+    int sx = (cx >= 0.0f) ? 1 : -1, sy = (cy >= 0.0f) ? 1 : -1;
+    int n = 0;
+    for (;;) {
+        float t;
+        ++n;
+        if (tMaxX < tMaxY) { t = tMaxX; ix += sx; tMaxX += dX; } else { t = tMaxY; iy += sy; tMaxY += dY; }
+        if ((unsigned)ix >= (unsigned)s->W || (unsigned)iy >= (unsigned)s->H) return n;
+        float zr = fmaf(cz, t, oz);
+        if (is_upper && zr > s->maxz) return n;
+        if (!is_upper && zr < 0.0f) return n;
+        if (s->grid[ix + iy * s->W] - zr > 0.01f) return n;
+    }
+}
+
+int orc_trace_steps(const float* grid, int W, int H, int num_total, int num_top,
+                    const int* pix_parent, const float* wall_z, float maxz,
+                    const float* dirs, const int* dense, const int* upper, int D,
+                    const int* voxels, int nv, short* steps)
+{
+    orc_scene s = { grid, W, H, num_total, num_top, pix_parent, wall_z, maxz, dirs, dense, upper, D, 1 };
+    for (int i = 0; i < nv; ++i)
+        for (int d = 0; d < D; ++d) {
+            int n = trace_ray_steps(&s, voxels[i], dirs[3 * d], dirs[3 * d + 1], dirs[3 * d + 2], upper[d]);
+            steps[(size_t)i * D + d] = (short)(n > 32767 ? 32767 : n);
+        }
+    return 0;
+}

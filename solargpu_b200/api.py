@@ -40,7 +40,8 @@ class SolarGPUError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("neighbor_format", C.c_int), ("hour_block", C.c_int), ("accumulation", C.c_int),
-                ("reflection", C.c_int), ("chunk_voxels", C.c_longlong), ("use_graph", C.c_int)]
+                ("reflection", C.c_int), ("chunk_voxels", C.c_longlong), ("use_graph", C.c_int),
+                ("time_kernels", C.c_int), ("group_size", C.c_int)]
 
 
 class SceneDesc(C.Structure):
@@ -80,6 +81,7 @@ def lib() -> C.CDLL:
         L.solar_gpu_trace_sizes.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.solar_gpu_trace_copy.argtypes = [vp, vp, vp, vp, vp, vp]
         L.solar_gpu_last_timings.argtypes = [vp, C.POINTER(C.c_double), i]
+        L.solar_gpu_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(ll), i]
         _LIB = L
     return _LIB
 
@@ -258,6 +260,17 @@ class Context:
         if n < 0:
             _check(n)
         return list(ms)[:n]
+
+    KERNEL_GROUPS = ("setup", "trace", "dedupe", "csr", "barle", "solar", "reflect", "finalize", "group")
+
+    def kernel_times(self) -> dict:
+        """{group: (ms, launches)} of the last run made with time_kernels=1."""
+        ms = (C.c_double * 9)()
+        ln = (C.c_longlong * 9)()
+        n = lib().solar_gpu_kernel_times(self.h, ms, ln, 9)
+        if n < 0:
+            _check(n)
+        return {g: (ms[i], int(ln[i])) for i, g in enumerate(self.KERNEL_GROUPS[:n])}
 
     def launches(self) -> int:
         return int(lib().solar_gpu_last_launch_count(self.h))

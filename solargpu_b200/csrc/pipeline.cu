@@ -57,6 +57,7 @@ struct DevBuf {
 
 template <typename T> T* as(DevBuf& b) { return static_cast<T*>(b.p); }
 
+
 __global__ void k_validate_parents(const int* __restrict__ pp, int N, int T, int* __restrict__ bad)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -75,7 +76,8 @@ struct solar_gpu_context {
     DevBuf dirs, nudged, dni, dhi, sun_dense, hour_index, table, geo_n, geo_p, shadow, raw,
         counts, csr_off, csr_ids, barle_off, barle_sizes, barle_bytes, scan_tmp, slab, hourly,
         acc_f64, acc_f32, acc_comp, sums, out_f64, err, in_grid, in_pp, in_wz, in_slopes,
-        in_aspects, out_f32;
+        in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
+        grp_cell, grp_w;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
@@ -83,7 +85,14 @@ struct solar_gpu_context {
     bool have_csr = false, have_barle = false;
     double timings[4] = {0, 0, 0, 0};
     long long launches = 0;
+    long long group_entries = 0;
     bool timed = false;
+    // per kernel-group event log (time_kernels)
+    bool ktime = false;
+    std::vector<cudaEvent_t> kt_pool;
+    std::vector<int> kt_ids;   // group of event pair i
+    int kt_used = 0;
+    cudaStream_t kt_stream = nullptr;
 };
 
 namespace {
@@ -124,6 +133,30 @@ int read_ll(solar_gpu_context* c, const long long* dev, long long* out, cudaStre
     return SOLAR_GPU_OK;
 }
 
+// Event pair around a kernel group when time_kernels is set.
+struct KScope {
+    solar_gpu_context* c;
+    int idx = -1;
+    KScope(solar_gpu_context* ctx, int group) : c(ctx)
+    {
+        if (!c->ktime) return;
+        if ((size_t)(2 * c->kt_used + 2) > c->kt_pool.size()) {
+            for (int i = 0; i < 256; ++i) {
+                cudaEvent_t e;
+                if (cudaEventCreate(&e) != cudaSuccess) return;
+                c->kt_pool.push_back(e);
+            }
+        }
+        idx = c->kt_used++;
+        c->kt_ids.push_back(group);
+        cudaEventRecord(c->kt_pool[2 * idx], c->kt_stream);
+    }
+    ~KScope()
+    {
+        if (idx >= 0) cudaEventRecord(c->kt_pool[2 * idx + 1], c->kt_stream);
+    }
+};
+
 int check_scene(const solar_gpu_scene* s)
 {
     if (!s) return fail(SOLAR_GPU_ERR_ARG, "scene is NULL");
@@ -154,6 +187,11 @@ int check_options(const solar_gpu_options* o, bool trace_only)
     if (o->accumulation < 0 || o->accumulation > 2) return fail(SOLAR_GPU_ERR_ARG, "accumulation %d", o->accumulation);
     if (o->reflection < 0 || o->reflection > 1) return fail(SOLAR_GPU_ERR_ARG, "reflection %d", o->reflection);
     if (o->chunk_voxels < 0) return fail(SOLAR_GPU_ERR_ARG, "chunk_voxels %lld", o->chunk_voxels);
+    if (!(o->group_size == 0 || o->group_size == 4 || o->group_size == 8))
+        return fail(SOLAR_GPU_ERR_ARG, "group_size %d (0, 4 or 8)", o->group_size);
+    const int Bq = B == 0 ? 128 : B;
+    if (Bq > 1 && ((o->group_size == 8 && Bq > 128) || (o->group_size == 4 && Bq > 256)))
+        return fail(SOLAR_GPU_ERR_ARG, "hour_block %d too wide for group_size %d", Bq, o->group_size);
     return SOLAR_GPU_OK;
 }
 
@@ -195,21 +233,40 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
     CK(cudaMemcpyAsync(c->sun_dense.p, sky.sun_dense.data(), sizeof(int) * kHoursPerYear, cudaMemcpyHostToDevice, st));
     if (Hd) CK(cudaMemcpyAsync(c->hour_index.p, sky.hour_index.data(), sizeof(int) * Hd, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int), st));
-    CK(launch_hour_table(as<float>(c->nudged), as<float>(c->dni), as<float>(c->dhi), as<int>(c->sun_dense),
-                         as<int>(c->hour_index), Hd, n_padded, as<HourEntry>(c->table), st));
+    {
+        KScope k(c, SOLAR_GPU_KT_SETUP);
+        CK(launch_hour_table(as<float>(c->nudged), as<float>(c->dni), as<float>(c->dhi), as<int>(c->sun_dense),
+                             as<int>(c->hour_index), Hd, n_padded, as<HourEntry>(c->table), st));
+    }
     const int N = s->num_total_voxels;
     RK(ensure(c->geo_n, sizeof(float4) * (size_t)N));
     RK(ensure(c->geo_p, sizeof(float4) * (size_t)N));
-    k_validate_parents<<<(N + 255) / 256, 256, 0, st>>>(s->pixel_parent, N, s->num_top_voxels, as<int>(c->err));
-    CK(cudaGetLastError());
+    {
+        KScope k(c, SOLAR_GPU_KT_SETUP);
+        k_validate_parents<<<(N + 255) / 256, 256, 0, st>>>(s->pixel_parent, N, s->num_top_voxels, as<int>(c->err));
+        CK(cudaGetLastError());
+    }
     int bad = 0;
     CK(cudaMemcpyAsync(c->h_scalars, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     std::memcpy(&bad, c->h_scalars, sizeof(int));
     if (bad) return fail(SOLAR_GPU_ERR_ARG, "pixel_parent violates the voxel layout (tops i -> i, walls in [0, T))");
     DevGeom g{as<float4>(c->geo_n), as<float4>(c->geo_p)};
-    CK(launch_voxel_geom(dev_scene(s), g, st));
-    c->launches += 3;
+    {
+        KScope k(c, SOLAR_GPU_KT_SETUP);
+        CK(launch_voxel_geom(dev_scene(s), g, st));
+    }
+    {
+        const long long npos = order_positions(s->grid_width, s->grid_height);
+        RK(ensure(c->order, sizeof(int) * (size_t)N));
+        RK(ensure(c->order_cnt, sizeof(int) * (size_t)npos));
+        RK(ensure(c->order_cur, sizeof(long long) * ((size_t)npos + 1)));
+        RK(ensure(c->order_tmp, sizeof(long long) * scan_scratch_elems((int)npos)));
+        KScope k(c, SOLAR_GPU_KT_SETUP);
+        CK(launch_voxel_order(s->pixel_parent, N, s->grid_width, s->grid_height, as<int>(c->order_cnt),
+                              as<long long>(c->order_cur), as<long long>(c->order_tmp), as<int>(c->order), st));
+    }
+    c->launches += 8;
     return SOLAR_GPU_OK;
 }
 
@@ -256,33 +313,51 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     long long csr_total = 0, barle_total = 0;
     for (long long v0 = 0; v0 < N; v0 += chunk) {
         const int n = (int)((N - v0) < chunk ? (N - v0) : chunk);
-        CK(launch_trace(ds, as<DirEntry>(c->dirs), D, c->words32, (int)v0, n, as<int>(c->raw),
-                        as<uint32_t>(c->shadow), st));
-        CK(launch_dedupe(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->err), st));
+        {
+            KScope k(c, SOLAR_GPU_KT_TRACE);
+            CK(launch_trace(ds, as<DirEntry>(c->dirs), D, c->words32, (int)v0, n, as<int>(c->raw),
+                            as<uint32_t>(c->shadow), st));
+        }
+        {
+            KScope k(c, SOLAR_GPU_KT_DEDUPE);
+            CK(launch_dedupe(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->err), st));
+        }
         c->launches += 2;
         const double frac_left = (double)N / (double)(v0 + n);
         if (want_csr) {
             long long* off = as<long long>(c->csr_off) + v0;
-            CK(launch_scan_counts(as<int>(c->counts) + v0, n, csr_total, off, as<long long>(c->scan_tmp), nullptr, st));
+            {
+                KScope k(c, SOLAR_GPU_KT_CSR);
+                CK(launch_scan_counts(as<int>(c->counts) + v0, n, csr_total, off, as<long long>(c->scan_tmp), nullptr, st));
+            }
             long long total = 0;
             RK(read_ll(c, off + n, &total, st));
             const long long est = (long long)(total * frac_left * 1.05);
             RK(ensure_keep(c->csr_ids, sizeof(int) * (size_t)(est > total ? est : total), sizeof(int) * (size_t)csr_total, st));
-            CK(launch_gather_csr(n, D, as<int>(c->raw), off, as<int>(c->csr_ids), st));
+            {
+                KScope k(c, SOLAR_GPU_KT_CSR);
+                CK(launch_gather_csr(n, D, as<int>(c->raw), off, as<int>(c->csr_ids), st));
+            }
             csr_total = total;
             c->launches += 4;
         }
         if (want_barle) {
             long long* off = as<long long>(c->barle_off) + v0;
-            CK(launch_barle_size(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->barle_sizes) + v0,
-                                 as<int>(c->err), st));
-            CK(launch_scan_counts(as<int>(c->barle_sizes) + v0, n, barle_total, off, as<long long>(c->scan_tmp), nullptr, st));
+            {
+                KScope k(c, SOLAR_GPU_KT_BARLE);
+                CK(launch_barle_size(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->barle_sizes) + v0,
+                                     as<int>(c->err), st));
+                CK(launch_scan_counts(as<int>(c->barle_sizes) + v0, n, barle_total, off, as<long long>(c->scan_tmp), nullptr, st));
+            }
             long long total = 0;
             RK(read_ll(c, off + n, &total, st));
             const long long est = (long long)(total * frac_left * 1.05);
             RK(ensure_keep(c->barle_bytes, (size_t)(est > total ? est : total), (size_t)barle_total, st));
-            CK(launch_barle_write(n, D, as<int>(c->raw), as<int>(c->counts) + v0, off,
-                                  as<unsigned char>(c->barle_bytes), as<int>(c->err), st));
+            {
+                KScope k(c, SOLAR_GPU_KT_BARLE);
+                CK(launch_barle_write(n, D, as<int>(c->raw), as<int>(c->counts) + v0, off,
+                                      as<unsigned char>(c->barle_bytes), as<int>(c->err), st));
+            }
             barle_total = total;
             c->launches += 5;
         }
@@ -316,9 +391,18 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
     if (o->reflection == SOLAR_GPU_REFL_ANNUAL) {
         RK(ensure(c->sums, sizeof(double) * (size_t)N));
         RK(ensure(c->out_f64, sizeof(double) * (size_t)N));
-        CK(launch_solar_sum(g, N, sh, c->words32, tab, Hd, as<double>(c->sums), st));
-        CK(launch_reflect_annual(g, N, T, as<double>(c->sums), nl, as<double>(c->out_f64), err, st));
-        CK(launch_finalize_f64(as<double>(c->out_f64), N, out, st));
+        {
+            KScope k(c, SOLAR_GPU_KT_SOLAR);
+            CK(launch_solar_sum(g, N, sh, c->words32, tab, Hd, as<double>(c->sums), st));
+        }
+        {
+            KScope k(c, SOLAR_GPU_KT_REFLECT);
+            CK(launch_reflect_annual(g, N, T, as<double>(c->sums), nl, as<double>(c->out_f64), err, st));
+        }
+        {
+            KScope k(c, SOLAR_GPU_KT_FINALIZE);
+            CK(launch_finalize_f64(as<double>(c->out_f64), N, out, st));
+        }
         c->launches += 3;
         return SOLAR_GPU_OK;
     }
@@ -341,22 +425,68 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
     if (B == 1) {
         RK(ensure(c->hourly, sizeof(float) * (size_t)N));
         for (int j = 0; j < Hd; ++j) {
-            CK(launch_solar_hour(g, N, sh, c->words32, tab, j, as<float>(c->hourly), st));
-            CK(launch_reflect_hour(g, N, T, as<float>(c->hourly), nl, acc, err, st));
+            {
+                KScope k(c, SOLAR_GPU_KT_SOLAR);
+                CK(launch_solar_hour(g, N, sh, c->words32, tab, j, as<float>(c->hourly), st));
+            }
+            {
+                KScope k(c, SOLAR_GPU_KT_REFLECT);
+                CK(launch_reflect_hour(g, N, T, as<float>(c->hourly), nl, acc, err, st));
+            }
         }
         c->launches += 2LL * Hd;
     } else {
         RK(ensure(c->slab, sizeof(float) * (size_t)T * B));
         float* slab = as<float>(c->slab);
+        GroupLists gl{o->group_size, nullptr, nullptr, nullptr};
+        if (o->group_size > 0) {
+            // merged weighted union lists of each group of V voxels (once per run)
+            const int V = o->group_size;
+            const int G = group_count(N, V);
+            RK(ensure(c->grp_cnt, sizeof(int) * (size_t)G));
+            RK(ensure(c->grp_off, sizeof(long long) * ((size_t)G + 1)));
+            RK(ensure(c->grp_tmp, sizeof(long long) * scan_scratch_elems(G)));
+            {
+                KScope k(c, SOLAR_GPU_KT_GROUP);
+                CK(launch_group_build(0, V, g, N, T, nl, as<int>(c->order), as<int>(c->grp_cnt), nullptr,
+                                      nullptr, nullptr, err, st));
+                CK(launch_scan_counts(as<int>(c->grp_cnt), G, 0, as<long long>(c->grp_off),
+                                      as<long long>(c->grp_tmp), nullptr, st));
+            }
+            long long E = 0;
+            RK(read_ll(c, as<long long>(c->grp_off) + G, &E, st));
+            RK(ensure(c->grp_cell, sizeof(int) * (size_t)(E + 1)));
+            RK(ensure(c->grp_w, sizeof(float) * (size_t)(E + 1) * V));
+            {
+                KScope k(c, SOLAR_GPU_KT_GROUP);
+                CK(launch_group_build(1, V, g, N, T, nl, as<int>(c->order), as<int>(c->grp_cnt),
+                                      as<long long>(c->grp_off), as<int>(c->grp_cell), as<float>(c->grp_w),
+                                      err, st));
+            }
+            c->group_entries = E;
+            c->launches += 5;
+            gl.offsets = as<long long>(c->grp_off);
+            gl.cells = as<int>(c->grp_cell);
+            gl.weights = as<float>(c->grp_w);
+        }
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
-        const bool use_graph = o->use_graph != 0;
+        const bool use_graph = o->use_graph != 0 && !c->ktime;
         if (use_graph) CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         cudaError_t le = cudaSuccess;
         for (int j0 = 0; j0 < Hd && le == cudaSuccess; j0 += B) {
-            le = launch_solar_slab(g, T, sh, c->words32, tab, j0, B, slab, st);
-            if (le == cudaSuccess)
-                le = launch_reflect_block(g, N, T, sh, c->words32, tab, j0, B, slab, nl, acc, err, st);
+            {
+                KScope k(c, SOLAR_GPU_KT_SOLAR);
+                le = launch_solar_slab(g, T, sh, c->words32, tab, j0, B, slab, st);
+            }
+            if (le == cudaSuccess) {
+                KScope k(c, SOLAR_GPU_KT_REFLECT);
+                if (o->group_size > 0)
+                    le = launch_reflect_group(g, N, sh, c->words32, tab, j0, B, slab, gl, as<int>(c->order), acc, st);
+                else
+                    le = launch_reflect_block(g, N, T, sh, c->words32, tab, j0, B, slab, nl, acc,
+                                              as<int>(c->order), err, st);
+            }
             c->launches += 2;
         }
         if (use_graph) {
@@ -369,7 +499,10 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         }
         CK(le);
     }
-    CK(launch_finalize(acc, N, out, st));
+    {
+        KScope k(c, SOLAR_GPU_KT_FINALIZE);
+        CK(launch_finalize(acc, N, out, st));
+    }
     c->launches += 1;
     return SOLAR_GPU_OK;
 }
@@ -393,6 +526,10 @@ int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const sola
     CK(cudaSetDevice(c->device));
     c->launches = 0;
     c->timed = false;
+    c->ktime = o->time_kernels != 0;
+    c->kt_used = 0;
+    c->kt_ids.clear();
+    c->kt_stream = st;
     CK(cudaEventRecord(c->ev[0], st));
     SkyTables sky;
     RK(prepare(c, s, sky, st));
@@ -455,6 +592,8 @@ void solar_gpu_default_options(solar_gpu_options* o)
     o->reflection = SOLAR_GPU_REFL_HOURLY;
     o->chunk_voxels = 0;
     o->use_graph = 1;
+    o->time_kernels = 0;
+    o->group_size = 8;
 }
 
 const char* solar_gpu_last_error(void) { return g_err.c_str(); }
@@ -487,9 +626,12 @@ void solar_gpu_destroy(solar_gpu_context* c)
                       &c->geo_n, &c->geo_p, &c->shadow, &c->raw, &c->counts, &c->csr_off, &c->csr_ids,
                       &c->barle_off, &c->barle_sizes, &c->barle_bytes, &c->scan_tmp, &c->slab, &c->hourly,
                       &c->acc_f64, &c->acc_f32, &c->acc_comp, &c->sums, &c->out_f64, &c->err, &c->in_grid,
-                      &c->in_pp, &c->in_wz, &c->in_slopes, &c->in_aspects, &c->out_f32};
+                      &c->in_pp, &c->in_wz, &c->in_slopes, &c->in_aspects, &c->out_f32, &c->order,
+                      &c->order_cnt, &c->order_cur, &c->order_tmp, &c->grp_cnt, &c->grp_off,
+                      &c->grp_tmp, &c->grp_cell, &c->grp_w};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (cudaEvent_t e : c->kt_pool) cudaEventDestroy(e);
     if (c->own) cudaStreamDestroy(c->own);
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     delete c;
@@ -589,6 +731,22 @@ int solar_gpu_last_timings(solar_gpu_context* c, double* ms, int n)
 }
 
 long long solar_gpu_last_launch_count(solar_gpu_context* c) { return c ? c->launches : -1; }
+
+int solar_gpu_kernel_times(solar_gpu_context* c, double* ms, long long* launches, int n)
+{
+    if (!c || !ms || !launches) return fail(SOLAR_GPU_ERR_ARG, "NULL argument");
+    const int k = n < SOLAR_GPU_KT_COUNT ? n : SOLAR_GPU_KT_COUNT;
+    for (int i = 0; i < k; ++i) { ms[i] = 0.0; launches[i] = 0; }
+    if (c->kt_used == 0) return k;
+    CK(cudaEventSynchronize(c->kt_pool[2 * (c->kt_used - 1) + 1]));
+    for (int i = 0; i < c->kt_used; ++i) {
+        float t = 0.0f;
+        CK(cudaEventElapsedTime(&t, c->kt_pool[2 * i], c->kt_pool[2 * i + 1]));
+        const int g = c->kt_ids[i];
+        if (g < k) { ms[g] += t; launches[g] += 1; }
+    }
+    return k;
+}
 
 int solar_gpu_uncompressed_gpu_irradiance(
     const float* grid_data, int grid_width, int grid_height, int num_total_voxels, int num_top_voxels,

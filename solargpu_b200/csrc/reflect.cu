@@ -71,24 +71,31 @@ __device__ __forceinline__ void barle_for_each_chunk(const unsigned char* __rest
         const int total_pay = __shfl_sync(kFull, pp, 7);
         const long long pay_base = cur + 3 + nc;
         if (pay_base + total_pay > size) { if (lane == 0) atomicOr(err, kErrBarleStream); return; }
-        if (lane < nc) runs[lane] = make_int4(w, len, lp - len, pp - pay);
-        __syncwarp();
+        // Run table in registers: lane r < 8 holds run r (lanes nc..7 hold
+        // empty runs starting at total_len, so they are never selected).
+        const int estart = lp - len, boff = pp - pay;
+        int st[7];
+#pragma unroll
+        for (int t = 0; t < 7; ++t) st[t] = __shfl_sync(kFull, estart, t + 1);
         const unsigned char* payload = bytes + base + pay_base;
         for (int e0 = 0; e0 < total_len; e0 += 32) {
             const int e = e0 + lane;
             const bool valid = e < total_len;
+            int r = 0;
+#pragma unroll
+            for (int t = 0; t < 7; ++t) r += (e >= st[t]) ? 1 : 0;
+            const int Rw = __shfl_sync(kFull, w, r);
+            const int Rs = __shfl_sync(kFull, estart, r);
+            const int Rb = __shfl_sync(kFull, boff, r);
             uint32_t d = 0;
             if (valid) {
-                int r = 0;
-                for (int t = 1; t < nc; ++t) if (runs[t].z <= e) r = t;
-                const int4 R = runs[r];
-                const int i = e - R.z;
-                const unsigned char* q = payload + R.w;
-                if (R.x == 0) {
+                const int i = e - Rs;
+                const unsigned char* q = payload + Rb;
+                if (Rw == 0) {
                     const uint32_t b = q[i >> 1];
                     d = (i & 1) ? (b & 15u) : (b >> 4);
                 } else {
-                    for (int b = 0; b < R.x; ++b) d = (d << 8) | q[i * R.x + b];
+                    for (int b = 0; b < Rw; ++b) d = (d << 8) | q[i * Rw + b];
                 }
             }
             uint32_t s = valid ? ((first && e == 0) ? d : 0u - d) : 0u;
@@ -119,6 +126,42 @@ __device__ __forceinline__ void csr_for_each_chunk(const long long* __restrict__
     }
 }
 
+// Hours of the block (B = 32*Q) owned by lane L: for Q <= 4 the Q contiguous
+// hours L*Q .. L*Q+Q-1 (one Q-wide vector load); for Q = 8 the hours
+// 4L .. 4L+3 and 128+4L .. 128+4L+3 (two float4 loads, each instruction a
+// contiguous 512-byte span).  A warp reads one whole slab row per neighbor.
+__device__ __forceinline__ int lane_hour(int Q, int lane, int q)
+{
+    return Q <= 4 ? lane * Q + q : 128 * (q >> 2) + 4 * lane + (q & 3);
+}
+
+template <int Q> struct SlabVec;
+template <> struct SlabVec<1> { using T = float; };
+template <> struct SlabVec<2> { using T = float2; };
+template <> struct SlabVec<4> { using T = float4; };
+template <> struct SlabVec<8> { using T = float4; };   // two float4 per lane
+
+template <int Q>
+__device__ __forceinline__ void fma_row(float (&acc)[Q], float w, const float* __restrict__ row, int lane)
+{
+    if constexpr (Q == 1) {
+        acc[0] = fmaf(w, __ldg(row + lane), acc[0]);
+    } else if constexpr (Q == 2) {
+        const float2 x = __ldg(reinterpret_cast<const float2*>(row) + lane);
+        acc[0] = fmaf(w, x.x, acc[0]);
+        acc[1] = fmaf(w, x.y, acc[1]);
+    } else {
+#pragma unroll
+        for (int h = 0; h < Q / 4; ++h) {
+            const float4 x = __ldg(reinterpret_cast<const float4*>(row) + lane + 32 * h);
+            acc[4 * h] = fmaf(w, x.x, acc[4 * h]);
+            acc[4 * h + 1] = fmaf(w, x.y, acc[4 * h + 1]);
+            acc[4 * h + 2] = fmaf(w, x.z, acc[4 * h + 2]);
+            acc[4 * h + 3] = fmaf(w, x.w, acc[4 * h + 3]);
+        }
+    }
+}
+
 template <int Q>
 __device__ __forceinline__ void slab_chunk(int g, const float4 me_p, const float4 me_n,
                                            const float4* __restrict__ geo_p, int T,
@@ -131,12 +174,10 @@ __device__ __forceinline__ void slab_chunk(int g, const float4 me_p, const float
     if (w != 0.0f) wg[__popc(bal & lanemask_lt(lane))] = make_float2(w, __int_as_float(g));
     __syncwarp();
     const int n = __popc(bal);
-#pragma unroll 4
+#pragma unroll 8
     for (int t = 0; t < n; ++t) {
         const float2 x = wg[t];
-        const float* row = slab + (size_t)__float_as_int(x.y) * (32 * Q) + lane;
-#pragma unroll
-        for (int q = 0; q < Q; ++q) acc[q] = fmaf(x.x, __ldg(row + 32 * q), acc[q]);
+        fma_row<Q>(acc, x.x, slab + (size_t)__float_as_int(x.y) * (32 * Q), lane);
     }
     __syncwarp();
 }
@@ -157,28 +198,31 @@ __device__ __forceinline__ void accumulate(const Accum& a, int v, float x)
     }
 }
 
+// Voxels are visited in `order` (tile-major, see k_tile_order), CTA b taking
+// groups of kReflWarps consecutive entries: the warps of a CTA hold nearby
+// voxels (shared slab rows in L1) and all CTAs together sweep a compact
+// window of the DSM (its slab rows stay in L2).
 template <int Q, int FMT>
 __global__ void __launch_bounds__(kReflWarps * 32)
 k_reflect_block(float4* __restrict__ geo_n_, float4* __restrict__ geo_p_, int N, int T,
                 const uint32_t* __restrict__ shadow, int words32, const HourEntry* __restrict__ table,
-                int j0, const float* __restrict__ slab, NeighborLists nl, Accum acc, int* err)
+                int j0, const float* __restrict__ slab, NeighborLists nl, Accum acc,
+                const int* __restrict__ order, int* err)
 {
     __shared__ float2 s_wg[kReflWarps][32];
     __shared__ int4 s_runs[kReflWarps][8];
     const float4* geo_n = geo_n_;
     const float4* geo_p = geo_p_;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int stride = gridDim.x * kReflWarps;
-    for (int v = blockIdx.x * kReflWarps + warp; v < N; v += stride) {
+    for (int grp = blockIdx.x; grp * kReflWarps < N; grp += gridDim.x) {
+        const int i = grp * kReflWarps + warp;
+        if (i >= N) continue;
+        const int v = order ? __ldg(order + i) : i;
         const float4 me_p = __ldg(geo_p + v);
         const float4 me_n = __ldg(geo_n + v);
-        float own[Q], r[Q];
+        float r[Q];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const HourEntry e = table[j0 + lane + 32 * q];
-            own[q] = solar_I(me_n, e, shadow_bit(shadow, words32, v, e.dense));
-            r[q] = 0.0f;
-        }
+        for (int q = 0; q < Q; ++q) r[q] = 0.0f;
         auto chunk = [&](int g) { slab_chunk<Q>(g, me_p, me_n, geo_p, T, s_wg[warp], slab, lane, r); };
         if (FMT == 0) {
             csr_for_each_chunk(nl.offsets, nl.ids, v, lane, chunk);
@@ -186,9 +230,13 @@ k_reflect_block(float4* __restrict__ geo_n_, float4* __restrict__ geo_p_, int N,
             const long long b0 = nl.offsets[v];
             barle_for_each_chunk(nl.bytes, b0, nl.offsets[v + 1] - b0, lane, s_runs[warp], err, chunk);
         }
+        // the voxel's own direct + diffuse for its hours, added to R
         float sum = 0.0f;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) sum += own[q] + r[q];
+        for (int q = 0; q < Q; ++q) {
+            const HourEntry e = table[j0 + lane_hour(Q, lane, q)];
+            sum += solar_I(me_n, e, shadow_bit(shadow, words32, v, e.dense)) + r[q];
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
         if (lane == 0) accumulate(acc, v, sum);
@@ -335,15 +383,15 @@ int refl_grid(int N)
 template <int Q>
 cudaError_t launch_block_q(const DevGeom& g, int N, int T, const uint32_t* shadow, int words32,
                            const HourEntry* table, int j0, const float* slab, const NeighborLists& nl,
-                           const Accum& acc, int* err, cudaStream_t st)
+                           const Accum& acc, const int* order, int* err, cudaStream_t st)
 {
     const int grid = refl_grid(N);
     if (nl.format == 0)
         k_reflect_block<Q, 0><<<grid, kReflWarps * 32, 0, st>>>(g.geo_n, g.geo_p, N, T, shadow, words32,
-                                                              table, j0, slab, nl, acc, err);
+                                                              table, j0, slab, nl, acc, order, err);
     else
         k_reflect_block<Q, 1><<<grid, kReflWarps * 32, 0, st>>>(g.geo_n, g.geo_p, N, T, shadow, words32,
-                                                              table, j0, slab, nl, acc, err);
+                                                              table, j0, slab, nl, acc, order, err);
     return cudaGetLastError();
 }
 
@@ -352,14 +400,14 @@ cudaError_t launch_block_q(const DevGeom& g, int N, int T, const uint32_t* shado
 cudaError_t launch_reflect_block(const DevGeom& g, int N, int T, const uint32_t* shadow,
                                  int words32, const HourEntry* table, int j0, int B,
                                  const float* slab, const NeighborLists& nl, const Accum& acc,
-                                 int* err, cudaStream_t st)
+                                 const int* order, int* err, cudaStream_t st)
 {
     if (N <= 0) return cudaSuccess;
     switch (B) {
-    case 32: return launch_block_q<1>(g, N, T, shadow, words32, table, j0, slab, nl, acc, err, st);
-    case 64: return launch_block_q<2>(g, N, T, shadow, words32, table, j0, slab, nl, acc, err, st);
-    case 128: return launch_block_q<4>(g, N, T, shadow, words32, table, j0, slab, nl, acc, err, st);
-    case 256: return launch_block_q<8>(g, N, T, shadow, words32, table, j0, slab, nl, acc, err, st);
+    case 32: return launch_block_q<1>(g, N, T, shadow, words32, table, j0, slab, nl, acc, order, err, st);
+    case 64: return launch_block_q<2>(g, N, T, shadow, words32, table, j0, slab, nl, acc, order, err, st);
+    case 128: return launch_block_q<4>(g, N, T, shadow, words32, table, j0, slab, nl, acc, order, err, st);
+    case 256: return launch_block_q<8>(g, N, T, shadow, words32, table, j0, slab, nl, acc, order, err, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -386,6 +434,70 @@ cudaError_t launch_reflect_annual(const DevGeom& g, int N, int T, const double* 
         k_reflect_annual<0><<<grid, kReflWarps * 32, 0, st>>>(g.geo_n, g.geo_p, N, T, sums, nl, out, err);
     else
         k_reflect_annual<1><<<grid, kReflWarps * 32, 0, st>>>(g.geo_n, g.geo_p, N, T, sums, nl, out, err);
+    return cudaGetLastError();
+}
+
+// Visiting order of the reflection pass: cells in 32 x 32 tiles (tiles in
+// serpentine row order, cells in Morton order inside a tile), each cell's
+// top voxel and walls together.  Built as a counting sort keyed by the cell
+// position in that order: count voxels per cell, exclusive scan, scatter
+// with per-cell cursors.  The order of walls inside a cell is arbitrary and
+// does not affect results (every voxel is reduced by its own warp).
+namespace {
+constexpr int kTileBits = 5;   // 32 x 32 cell tiles
+
+__device__ __forceinline__ unsigned spread5(unsigned x)
+{
+    x &= 31u;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+
+__device__ __forceinline__ long long cell_pos(int c, int W, int ntx)
+{
+    const int x = c % W, y = c / W;
+    const int tx = x >> kTileBits, ty = y >> kTileBits;
+    const long long tile = (long long)ty * ntx + ((ty & 1) ? (ntx - 1 - tx) : tx);
+    return (tile << (2 * kTileBits)) | (spread5((unsigned)x) | (spread5((unsigned)y) << 1));
+}
+
+__global__ void k_order_count(const int* __restrict__ pp, int N, int W, int ntx, int* __restrict__ cnt)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < N) atomicAdd(cnt + cell_pos(pp[v], W, ntx), 1);
+}
+
+__global__ void k_order_scatter(const int* __restrict__ pp, int N, int W, int ntx,
+                                unsigned long long* __restrict__ cursor, int* __restrict__ order)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < N) order[atomicAdd(cursor + cell_pos(pp[v], W, ntx), 1ull)] = v;
+}
+}  // namespace
+
+long long order_positions(int W, int H)
+{
+    const long long ntx = (W + (1 << kTileBits) - 1) >> kTileBits;
+    const long long nty = (H + (1 << kTileBits) - 1) >> kTileBits;
+    return ntx * nty << (2 * kTileBits);
+}
+
+cudaError_t launch_voxel_order(const int* pix_parent, int N, int W, int H, int* counts,
+                               long long* cursor, long long* scan_tmp, int* order, cudaStream_t st)
+{
+    if (N <= 0) return cudaSuccess;
+    const int ntx = (W + (1 << kTileBits) - 1) >> kTileBits;
+    const long long npos = order_positions(W, H);
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * npos, st);
+    if (e != cudaSuccess) return e;
+    k_order_count<<<(N + 255) / 256, 256, 0, st>>>(pix_parent, N, W, ntx, counts);
+    e = launch_scan_counts(counts, (int)npos, 0, cursor, scan_tmp, nullptr, st);
+    if (e != cudaSuccess) return e;
+    k_order_scatter<<<(N + 255) / 256, 256, 0, st>>>(pix_parent, N, W, ntx,
+                                                    reinterpret_cast<unsigned long long*>(cursor), order);
     return cudaGetLastError();
 }
 

@@ -63,8 +63,12 @@ CITY_1024 = DsmConfig("dsm1024", 1024, 150, 4600, seed=1024)
 CITY_4096 = DsmConfig("dsm4096", 4096, 2400, 130000, roof_max=60.0, seed=4096)
 # Mid-size case used by parity tests that must finish in seconds on the CPU oracle.
 TOWN_160 = DsmConfig("dsm160", 160, 20, 60, seed=160)
+# 256x256 and 512x512 cuts of the 1024 city's densities (profiling runs that
+# must stay small; at 512 the hour-block slab no longer fits in L2).
+CITY_256 = DsmConfig("dsm256", 256, 10, 290, seed=256)
+CITY_512 = DsmConfig("dsm512", 512, 38, 1150, seed=512)
 
-CONFIGS = {c.name: c for c in (SMALL_64, TOWN_160, CITY_1024, CITY_4096)}
+CONFIGS = {c.name: c for c in (SMALL_64, TOWN_160, CITY_256, CITY_512, CITY_1024, CITY_4096)}
 
 
 # --------------------------------------------------------------------------

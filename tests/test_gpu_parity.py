@@ -70,17 +70,21 @@ def test_trace_matches_reference_kernel(ctx, scene64):
     np.testing.assert_array_equal(r["shadow"], O.svf_to_words32(ref["svf"], r["shadow_words"]))
 
 
-CASES = [(fmt, B, acc) for fmt in (0, 1) for B in (1, 32, 64, 128, 256) for acc in (0, 1, 2)
-         if not (B == 1 and acc == 1 and fmt == 1)]
+# (format, hour block, accumulation, group size): the plain per-hour path,
+# the per-voxel block kernel (group 0) and the grouped kernel (4, 8).
+CASES = ([(fmt, 1, acc, 0) for fmt in (0, 1) for acc in (0, 1, 2)]
+         + [(fmt, B, acc, 0) for fmt in (0, 1) for B in (32, 64, 128, 256) for acc in (0, 1, 2)]
+         + [(fmt, B, acc, V) for fmt in (0, 1) for V in (4, 8) for B in (32, 64, 128, 256) for acc in (0, 1, 2)
+            if not (V == 8 and B == 256)])
 
 
-@pytest.mark.parametrize("fmt,B,acc", CASES)
-def test_irradiance_vs_fp64(ctx, scene64, fmt, B, acc):
+@pytest.mark.parametrize("fmt,B,acc,V", CASES)
+def test_irradiance_vs_fp64(ctx, scene64, fmt, B, acc, V):
     import torch
     s = scene64
     want = fp64_reference(s)
     out = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
-    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, hour_block=B, accumulation=acc)
+    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, hour_block=B, accumulation=acc, group_size=V)
     torch.cuda.synchronize()
     e = rel_err(out.cpu().numpy(), want)
     assert e.max() <= REL_TOL, (e.max(), e.mean())
@@ -98,13 +102,13 @@ def test_annual_form_vs_fp64(ctx, scene160, fmt):
     assert e.max() <= REL_TOL, (e.max(), e.mean())
 
 
-@pytest.mark.parametrize("fmt", [0, 1])
-def test_hour_block_vs_fp64_dsm160(ctx, scene160, fmt):
+@pytest.mark.parametrize("fmt,V", [(0, 0), (1, 0), (0, 8), (1, 8), (1, 4)])
+def test_hour_block_vs_fp64_dsm160(ctx, scene160, fmt, V):
     import torch
     s = scene160
     want = fp64_reference(s)
     out = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
-    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, hour_block=128)
+    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, hour_block=128, group_size=V)
     torch.cuda.synchronize()
     e = rel_err(out.cpu().numpy(), want)
     assert e.max() <= REL_TOL, (e.max(), e.mean())
@@ -143,6 +147,27 @@ def test_drop_in_vs_reference_api(cuda_lib, scene64, compressed):
     assert e_ours.max() <= REL_TOL
     assert rel_err(out, ref.astype(np.float64)).max() <= max(2 * REL_TOL, 2 * e_ref.max())
     assert e_ours.mean() <= e_ref.mean() * 1.01 + 1e-9
+
+
+def test_grouped_results_are_reproducible(ctx, scene160):
+    """Union entries are built in a fixed order, so runs are bit-identical."""
+    import torch
+    dev = device_arrays(scene160)
+    outs = []
+    for _ in range(2):
+        out = torch.zeros(scene160.num_total, dtype=torch.float32, device="cuda:0")
+        ctx.run_device(scene160, dev, out, neighbor_format=1, hour_block=128, group_size=8)
+        outs.append(out.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_invalid_hour_block_for_group_is_rejected(ctx, scene64):
+    import torch
+    from solargpu_b200 import api
+    out = torch.zeros(scene64.num_total, dtype=torch.float32, device="cuda:0")
+    with pytest.raises(api.SolarGPUError) as e:
+        ctx.run_device(scene64, device_arrays(scene64), out, hour_block=256, group_size=8)
+    assert e.value.code == -1
 
 
 def test_invalid_pixel_parent_is_rejected(ctx, scene64):
