@@ -173,6 +173,26 @@ int solar_gpu_kernel_times(solar_gpu_context* ctx, double* ms, long long* launch
 /* Number of kernel launches the library issued in the last run. */
 long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
 
+/* ---- encoding without device allocation -------------------------------- */
+
+/* No counterpart in the reference.  ba-RLE-encodes num_lists CSR neighbor
+   lists (device csr_offsets [num_lists+1] int64 from 0, device csr_ids
+   int32) into device barle_offsets [num_lists+1] and device barle_bytes
+   (capacity barle_capacity bytes); *barle_total (host) receives the byte
+   count, also when the capacity is too small (nothing is written then).
+   Bytes are identical to the library's own ba-RLE lists and to the reference
+   encoder.  For callers that may not allocate device memory (their GPU memory
+   is owned by a host framework's pool, or cudaMalloc/cudaFree stalls are not
+   acceptable): it allocates nothing; its scratch is one fixed static device
+   array of about 10.6 MB per device, so num_lists <= 1024 and each list
+   <= 2592 ids.  Calls share that array: calls that overlap on the GPU race
+   and must be serialised.  The first call on a device looks up the array's
+   address; make it before any stream capture.  Runs on `stream` (NULL = the
+   legacy default stream) and synchronises it. */
+int solar_gpu_barle_encode_noalloc(const long long* csr_offsets, const int* csr_ids, int num_lists,
+                                   long long* barle_offsets, unsigned char* barle_bytes,
+                                   long long barle_capacity, long long* barle_total, void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* solar_gpu_last_error(void);
 

@@ -69,6 +69,11 @@ __global__ void k_validate_parents(const int* __restrict__ pp, int N, int T, int
 
 }  // namespace
 
+namespace sgb {
+// Lets other translation units report through solar_gpu_last_error().
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace sgb
+
 struct solar_gpu_context {
     int device = 0;
     cudaStream_t own = nullptr;

@@ -59,6 +59,9 @@ struct DevGeom {
     float4* geo_p;
 };
 
+// Sets the calling thread's message returned by solar_gpu_last_error().
+void set_last_error(const char* msg);
+
 // ------------------------------------------------------------------ launchers
 
 // tracer (trace.cu)
