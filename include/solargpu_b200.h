@@ -48,7 +48,7 @@ enum { SOLAR_GPU_REFL_HOURLY = 0, SOLAR_GPU_REFL_ANNUAL = 1 };
 
 typedef struct solar_gpu_options {
     int neighbor_format;     /* SOLAR_GPU_CSR / SOLAR_GPU_BARLE (SOLAR_GPU_BOTH: trace only) */
-    int hour_block;          /* 1 = plain per-hour path; 32, 64, 128, 256 = hour-block SpMM width; 0 = default (128) */
+    int hour_block;          /* 1 = plain per-hour path; 32..512 = hour-block width (powers of 2); 0 = 128 */
     int accumulation;        /* SOLAR_GPU_ACC_* */
     int reflection;          /* SOLAR_GPU_REFL_HOURLY (reflection per hour, reference semantics) or
                                 SOLAR_GPU_REFL_ANNUAL (sum over hours first, one sparse product) */
@@ -57,9 +57,10 @@ typedef struct solar_gpu_options {
     int time_kernels;        /* record CUDA events around every kernel group (no graph); see
                                 solar_gpu_kernel_times */
     int group_size;          /* hour-block reflection kernel: 0 = one warp per voxel, list decoded
-                                in every block; 4 or 8 = voxels sharing one warp, their lists
-                                merged once per run into weighted union entries (hour_block <= 128
-                                for 8, <= 256 for 4) */
+                                and weights computed in every block (B 32..256); 1 = weights computed
+                                once per run (B 64..512); 2, 4, 8 = that many voxels share one warp,
+                                their weighted lists merged once per run into union entries
+                                (B 64..512, 32..256, 32..128) */
 } solar_gpu_options;
 
 void solar_gpu_default_options(solar_gpu_options* opt);

@@ -19,9 +19,11 @@
 namespace sgb {
 namespace {
 
-constexpr int kEncWarps = 4;
+constexpr int kEncWarps = 4;        // large instance
 constexpr int kIdsCap = 4096;
 constexpr int kRunsCap = 2624;
+constexpr int kSmallWarps = 8;      // small instance
+constexpr int kSmallIds = 1024;
 constexpr int kW4 = 0, kEnd = 7;
 
 __device__ __forceinline__ int width_class(uint32_t x)
@@ -140,19 +142,24 @@ __device__ int load_sorted(const int* row, int k, uint32_t* ids, int lane, bool 
     return n2;
 }
 
-__global__ void __launch_bounds__(kEncWarps * 32)
+// Two instances per pass: the small one (lists <= kSmallIds ids, 8 KB of
+// shared memory per warp, 8 warps per block) takes almost every voxel; the
+// large one takes only the longer lists (up to one id per direction).
+template <int IDS, int RUNS, int WARPS, bool LARGE>
+__global__ void __launch_bounds__(WARPS * 32)
 k_barle_size(int chunk_count, int D, int* __restrict__ raw, const int* __restrict__ counts,
              int* __restrict__ sizes, int* __restrict__ err)
 {
     extern __shared__ uint32_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t* ids = smem + warp * (kIdsCap + kRunsCap);
-    uint32_t* runs = ids + kIdsCap;
-    const int lv = blockIdx.x * kEncWarps + warp;
+    uint32_t* ids = smem + warp * (IDS + RUNS);
+    uint32_t* runs = ids + IDS;
+    const int lv = blockIdx.x * WARPS + warp;
     if (lv >= chunk_count) return;
     const int k = counts[lv];
+    if (LARGE != (k > kSmallIds)) return;
     if (k <= 0) { if (lane == 0) sizes[lv] = 0; return; }
-    if (k > D || k > kRunsCap) { if (lane == 0) { sizes[lv] = 0; atomicOr(err, kErrListCapacity); } return; }
+    if (k > D || k > RUNS) { if (lane == 0) { sizes[lv] = 0; atomicOr(err, kErrListCapacity); } return; }
     int* row = raw + (size_t)lv * D;
     load_sorted(row, k, ids, lane, true);
     for (int i = lane; i < k; i += 32) row[i] = (int)ids[i];   // keep the sorted list for the write pass
@@ -172,19 +179,21 @@ k_barle_size(int chunk_count, int D, int* __restrict__ raw, const int* __restric
     if (lane == 0) sizes[lv] = 3 * ((pieces + 7) / 8) + pieces + payload;
 }
 
-__global__ void __launch_bounds__(kEncWarps * 32)
+template <int IDS, int RUNS, int WARPS, bool LARGE>
+__global__ void __launch_bounds__(WARPS * 32)
 k_barle_write(int chunk_count, int D, const int* __restrict__ raw, const int* __restrict__ counts,
               const long long* __restrict__ offsets, unsigned char* __restrict__ out,
               int* __restrict__ err)
 {
     extern __shared__ uint32_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t* ids = smem + warp * (kIdsCap + kRunsCap);
-    uint32_t* runs = ids + kIdsCap;
-    const int lv = blockIdx.x * kEncWarps + warp;
+    uint32_t* ids = smem + warp * (IDS + RUNS);
+    uint32_t* runs = ids + IDS;
+    const int lv = blockIdx.x * WARPS + warp;
     if (lv >= chunk_count) return;
     const int k = counts[lv];
-    if (k <= 0 || k > D || k > kRunsCap) return;
+    if (LARGE != (k > kSmallIds)) return;
+    if (k <= 0 || k > D || k > RUNS) return;
     const int* row = raw + (size_t)lv * D;
     load_sorted(row, k, ids, lane, false);   // already sorted by k_barle_size
     int nr = build_runs(ids, k, runs, lane);
@@ -252,17 +261,38 @@ k_barle_write(int chunk_count, int D, const int* __restrict__ raw, const int* __
 
 }  // namespace
 
-static size_t enc_smem() { return (size_t)kEncWarps * (kIdsCap + kRunsCap) * sizeof(uint32_t); }
+template <int IDS, int RUNS, int WARPS, bool LARGE>
+cudaError_t size_pass(int chunk_count, int D, int* raw, const int* counts, int* sizes, int* err, cudaStream_t st)
+{
+    const size_t smem = (size_t)WARPS * (IDS + RUNS) * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(k_barle_size<IDS, RUNS, WARPS, LARGE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_barle_size<IDS, RUNS, WARPS, LARGE><<<(chunk_count + WARPS - 1) / WARPS, WARPS * 32, smem, st>>>(
+        chunk_count, D, raw, counts, sizes, err);
+    return cudaGetLastError();
+}
+
+template <int IDS, int RUNS, int WARPS, bool LARGE>
+cudaError_t write_pass(int chunk_count, int D, const int* raw, const int* counts, const long long* offsets,
+                       unsigned char* out, int* err, cudaStream_t st)
+{
+    const size_t smem = (size_t)WARPS * (IDS + RUNS) * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(k_barle_write<IDS, RUNS, WARPS, LARGE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_barle_write<IDS, RUNS, WARPS, LARGE><<<(chunk_count + WARPS - 1) / WARPS, WARPS * 32, smem, st>>>(
+        chunk_count, D, raw, counts, offsets, out, err);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_barle_size(int chunk_count, int D, int* raw, const int* counts,
                               int* sizes, int* err, cudaStream_t st)
 {
     if (chunk_count <= 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_barle_size, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem());
+    cudaError_t e = size_pass<kSmallIds, kSmallIds, kSmallWarps, false>(chunk_count, D, raw, counts, sizes, err, st);
     if (e != cudaSuccess) return e;
-    k_barle_size<<<(chunk_count + kEncWarps - 1) / kEncWarps, kEncWarps * 32, enc_smem(), st>>>(
-        chunk_count, D, raw, counts, sizes, err);
-    return cudaGetLastError();
+    return size_pass<kIdsCap, kRunsCap, kEncWarps, true>(chunk_count, D, raw, counts, sizes, err, st);
 }
 
 cudaError_t launch_barle_write(int chunk_count, int D, const int* raw, const int* counts,
@@ -270,11 +300,10 @@ cudaError_t launch_barle_write(int chunk_count, int D, const int* raw, const int
                                cudaStream_t st)
 {
     if (chunk_count <= 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_barle_write, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem());
+    cudaError_t e = write_pass<kSmallIds, kSmallIds, kSmallWarps, false>(chunk_count, D, raw, counts, offsets,
+                                                                         out, err, st);
     if (e != cudaSuccess) return e;
-    k_barle_write<<<(chunk_count + kEncWarps - 1) / kEncWarps, kEncWarps * 32, enc_smem(), st>>>(
-        chunk_count, D, raw, counts, offsets, out, err);
-    return cudaGetLastError();
+    return write_pass<kIdsCap, kRunsCap, kEncWarps, true>(chunk_count, D, raw, counts, offsets, out, err, st);
 }
 
 }  // namespace sgb

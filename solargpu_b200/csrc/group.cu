@@ -27,12 +27,12 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kBuildWarps = 4;
-constexpr int kBuildCap = 4096;        // (g, slot, w) triples per group held in shared memory
+constexpr int kBuildCap = 2048;        // (cell, slot, w) triples per group held in shared memory
 constexpr int kGroupWarps = 8;
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
-// ---- list iteration (duplicated from the per-block kernel's helpers) ------
+// ---- list iteration (same decoder as the per-block kernel in reflect.cu) ----
 
 template <typename F>
 __device__ __forceinline__ void csr_chunks(const long long* __restrict__ off, const int* __restrict__ ids,
@@ -135,15 +135,46 @@ __device__ __forceinline__ void list_chunks(const NeighborLists& nl, int v, int 
 }
 
 // ---- build ------------------------------------------------------------------
+//
+// Phase A (one warp per voxel, no shared memory): the nonzero weights of
+// each voxel's list, in visiting order p = 0..N-1 -> weighted lists
+// (cell, w) at woff[p].  With V = 1 these are the union entries.
+// Phase B (V > 1, one warp per group): the entries of the group's V voxels
+// are contiguous in the weighted lists; they are sorted by (cell, slot) in
+// shared memory and merged into entries {cell, w[0..V-1]}.
 
-// PASS 0: counts[q] = union entries of group q.  PASS 1: writes them at
-// offsets[q].  One warp per group; V voxels order[V*q .. V*q+V-1].
-template <int FMT, int PASS, int V>
+template <int FMT, int PASS>
+__global__ void __launch_bounds__(256)
+k_wlist(const float4* __restrict__ geo_n, const float4* __restrict__ geo_p, int N, int T,
+        NeighborLists nl, const int* __restrict__ order, int* __restrict__ counts,
+        const long long* __restrict__ woff, int* __restrict__ cells, float* __restrict__ wts, int* err)
+{
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p >= N) return;
+    const int v = order[p];
+    const float4 me_p = __ldg(geo_p + v), me_n = __ldg(geo_n + v);
+    long long e = PASS == 1 ? woff[p] : 0;
+    list_chunks<FMT>(nl, v, lane, err, [&](int g) {
+        float w = 0.0f;
+        if (g >= 0 && g < T) w = refl_weight(me_p, me_n, __ldg(geo_p + g));
+        const unsigned bal = __ballot_sync(kFull, w != 0.0f);
+        if (PASS == 1 && w != 0.0f) {
+            const long long o = e + __popc(bal & lanemask_lt(lane));
+            cells[o] = g;
+            wts[o] = w;
+        }
+        e += __popc(bal);
+    });
+    if (PASS == 0 && lane == 0) counts[p] = (int)e;
+}
+
+// PASS 0: counts[q] = union entries of group q.  PASS 1: writes them at goff[q].
+template <int V, int PASS>
 __global__ void __launch_bounds__(kBuildWarps * 32)
-k_group_build(const float4* __restrict__ geo_n, const float4* __restrict__ geo_p, int N, int T,
-              NeighborLists nl, const int* __restrict__ order, int* __restrict__ counts,
-              const long long* __restrict__ offsets, int* __restrict__ cell_out,
-              float* __restrict__ w_out, int* err)
+k_group_merge(int N, const long long* __restrict__ woff, const int* __restrict__ wcell,
+              const float* __restrict__ wts, int* __restrict__ counts, const long long* __restrict__ goff,
+              int* __restrict__ cell_out, float* __restrict__ w_out)
 {
     extern __shared__ uint32_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -152,59 +183,40 @@ k_group_build(const float4* __restrict__ geo_n, const float4* __restrict__ geo_p
     const int q = blockIdx.x * kBuildWarps + warp;
     const int G = (N + V - 1) / V;
     if (q >= G) return;
-    const int gs = min(V, N - q * V);
-
-    // gather nonzero weights into shared memory
-    int n = 0;
-    bool overflow = false;
-    for (int s = 0; s < gs; ++s) {
-        const int v = order[q * V + s];
-        const float4 me_p = __ldg(geo_p + v), me_n = __ldg(geo_n + v);
-        list_chunks<FMT>(nl, v, lane, err, [&](int g) {
-            float w = 0.0f;
-            if (g >= 0 && g < T) w = refl_weight(me_p, me_n, __ldg(geo_p + g));
-            const unsigned bal = __ballot_sync(kFull, w != 0.0f);
-            const int pos = n + __popc(bal & lanemask_lt(lane));
-            if (w != 0.0f && pos < kBuildCap) {
-                keys[pos] = ((uint32_t)g << 3) | (uint32_t)s;
-                vals[pos] = w;
-            }
-            n += __popc(bal);
-        });
-    }
-    overflow = n > kBuildCap;
-    __syncwarp();
-
-    if (overflow) {
-        // Unmerged: one entry per nonzero (voxel, neighbor), in list order.
-        if (PASS == 0) {
-            if (lane == 0) counts[q] = n;
-            return;
-        }
-        long long e = offsets[q];
-        for (int s = 0; s < gs; ++s) {
-            const int v = order[q * V + s];
-            const float4 me_p = __ldg(geo_p + v), me_n = __ldg(geo_n + v);
-            list_chunks<FMT>(nl, v, lane, err, [&](int g) {
-                float w = 0.0f;
-                if (g >= 0 && g < T) w = refl_weight(me_p, me_n, __ldg(geo_p + g));
-                const unsigned bal = __ballot_sync(kFull, w != 0.0f);
-                if (w != 0.0f) {
-                    const long long o = e + __popc(bal & lanemask_lt(lane));
-                    cell_out[o] = g;
+    const int p0 = q * V, gs = min(V, N - p0);
+    long long bnd[V + 1];
 #pragma unroll
-                    for (int t = 0; t < V; ++t) w_out[o * V + t] = (t == s) ? w : 0.0f;
-                }
-                e += __popc(bal);
-            });
+    for (int s = 0; s <= V; ++s) bnd[s] = woff[p0 + min(s, gs)];
+    const long long e0 = bnd[0];
+    const int n = (int)(bnd[V] - e0);
+    if (n > kBuildCap) {
+        // Too many for shared memory: unmerged, one nonzero weight per entry.
+        if (PASS == 0) { if (lane == 0) counts[q] = n; return; }
+        const long long o0 = goff[q];
+        for (int i = lane; i < n; i += 32) {
+            int s = 0;
+#pragma unroll
+            for (int t = 1; t < V; ++t) s += (e0 + i >= bnd[t]) ? 1 : 0;
+            cell_out[o0 + i] = wcell[e0 + i];
+#pragma unroll
+            for (int t = 0; t < V; ++t) w_out[(o0 + i) * V + t] = (t == s) ? wts[e0 + i] : 0.0f;
         }
         return;
     }
-
-    // sort the triples by key (cell, slot): bitonic over n2 = pow2 >= max(n, 32)
     int n2 = 32;
     while (n2 < n) n2 <<= 1;
-    for (int i = n + lane; i < n2; i += 32) { keys[i] = 0xFFFFFFFFu; vals[i] = 0.0f; }
+    for (int i = lane; i < n2; i += 32) {
+        if (i < n) {
+            int s = 0;
+#pragma unroll
+            for (int t = 1; t < V; ++t) s += (e0 + i >= bnd[t]) ? 1 : 0;
+            keys[i] = ((uint32_t)wcell[e0 + i] << 3) | (uint32_t)s;
+            vals[i] = wts[e0 + i];
+        } else {
+            keys[i] = 0xFFFFFFFFu;
+            vals[i] = 0.0f;
+        }
+    }
     __syncwarp();
     for (int size = 2; size <= n2; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
@@ -221,7 +233,6 @@ k_group_build(const float4* __restrict__ geo_n, const float4* __restrict__ geo_p
             __syncwarp();
         }
     }
-    // union entries = runs of equal cell
     if (PASS == 0) {
         int distinct = 0;
         for (int i0 = 0; i0 < n; i0 += 32) {
@@ -232,20 +243,19 @@ k_group_build(const float4* __restrict__ geo_n, const float4* __restrict__ geo_p
         if (lane == 0) counts[q] = distinct;
         return;
     }
-    const long long e0 = offsets[q];
-    const long long ne = offsets[q + 1] - e0;
-    for (long long i = lane; i < ne * V; i += 32) w_out[e0 * V + i] = 0.0f;
+    const long long o0 = goff[q];
+    const long long ne = goff[q + 1] - o0;
+    for (long long i = lane; i < ne * V; i += 32) w_out[o0 * V + i] = 0.0f;
     __syncwarp();
     int run = -1;
     for (int i0 = 0; i0 < n; i0 += 32) {
         const int i = i0 + lane;
         const bool head = i < n && (i == 0 || (keys[i] >> 3) != (keys[i - 1] >> 3));
         const unsigned bal = __ballot_sync(kFull, head);
-        // inclusive rank of this element's run
         const int r = run + __popc(bal & (lanemask_lt(lane) | (1u << lane)));
         if (i < n) {
-            if (head) cell_out[e0 + r] = (int)(keys[i] >> 3);
-            w_out[(e0 + r) * V + (keys[i] & 7u)] = vals[i];
+            if (head) cell_out[o0 + r] = (int)(keys[i] >> 3);
+            w_out[(o0 + r) * V + (keys[i] & 7u)] = vals[i];
         }
         run += __popc(bal);
     }
@@ -312,21 +322,31 @@ k_reflect_group(const float4* __restrict__ geo_n, int N, const uint32_t* __restr
             const int m = (int)min(32LL, e1 - c);
             if (lane < m) {
                 s_cell[warp][lane] = __ldg(gcell + c + lane);
-                const float4* src = reinterpret_cast<const float4*>(gw + (c + lane) * V);
+                if constexpr (V >= 4) {
+                    const float4* src = reinterpret_cast<const float4*>(gw + (c + lane) * V);
 #pragma unroll
-                for (int t = 0; t < V / 4; ++t)
-                    reinterpret_cast<float4*>(s_w[warp][lane])[t] = __ldg(src + t);
+                    for (int t = 0; t < V / 4; ++t)
+                        reinterpret_cast<float4*>(s_w[warp][lane])[t] = __ldg(src + t);
+                } else {
+#pragma unroll
+                    for (int t = 0; t < V; ++t) s_w[warp][lane][t] = __ldg(gw + (c + lane) * V + t);
+                }
             }
             __syncwarp();
-#pragma unroll 2
+#pragma unroll (V <= 1 ? 8 : V == 2 ? 4 : 2)
             for (int t = 0; t < m; ++t) {
                 float x[Q];
                 load_row<Q>(x, slab + (size_t)s_cell[warp][t] * (32 * Q), lane);
                 float w[V];
+                if constexpr (V >= 4) {
 #pragma unroll
-                for (int u = 0; u < V / 4; ++u) {
-                    const float4 ww = reinterpret_cast<const float4*>(s_w[warp][t])[u];
-                    w[4 * u] = ww.x; w[4 * u + 1] = ww.y; w[4 * u + 2] = ww.z; w[4 * u + 3] = ww.w;
+                    for (int u = 0; u < V / 4; ++u) {
+                        const float4 ww = reinterpret_cast<const float4*>(s_w[warp][t])[u];
+                        w[4 * u] = ww.x; w[4 * u + 1] = ww.y; w[4 * u + 2] = ww.z; w[4 * u + 3] = ww.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < V; ++u) w[u] = s_w[warp][t][u];
                 }
 #pragma unroll
                 for (int s = 0; s < V; ++s)
@@ -367,29 +387,18 @@ int sm_count()
     return sms;
 }
 
-template <int FMT, int PASS, int V>
-cudaError_t build_pass(const DevGeom& g, int N, int T, const NeighborLists& nl, const int* order,
-                       int* counts, const long long* offsets, int* cell, float* w, int* err, cudaStream_t st)
+template <int V, int PASS>
+cudaError_t merge_pass(int N, const long long* woff, const int* wcell, const float* wts, int* counts,
+                       const long long* goff, int* cell, float* w, cudaStream_t st)
 {
     const size_t smem = (size_t)kBuildWarps * 2 * kBuildCap * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute(k_group_build<FMT, PASS, V>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_group_merge<V, PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     const int G = (N + V - 1) / V;
-    k_group_build<FMT, PASS, V><<<(G + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, smem, st>>>(
-        g.geo_n, g.geo_p, N, T, nl, order, counts, offsets, cell, w, err);
+    k_group_merge<V, PASS><<<(G + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, smem, st>>>(
+        N, woff, wcell, wts, counts, goff, cell, w);
     return cudaGetLastError();
-}
-
-template <int V>
-cudaError_t build_v(int pass, const DevGeom& g, int N, int T, const NeighborLists& nl, const int* order,
-                    int* counts, const long long* offsets, int* cell, float* w, int* err, cudaStream_t st)
-{
-    if (nl.format == 0)
-        return pass == 0 ? build_pass<0, 0, V>(g, N, T, nl, order, counts, offsets, cell, w, err, st)
-                         : build_pass<0, 1, V>(g, N, T, nl, order, counts, offsets, cell, w, err, st);
-    return pass == 0 ? build_pass<1, 0, V>(g, N, T, nl, order, counts, offsets, cell, w, err, st)
-                     : build_pass<1, 1, V>(g, N, T, nl, order, counts, offsets, cell, w, err, st);
 }
 
 template <int Q, int V>
@@ -399,7 +408,7 @@ cudaError_t group_q(const DevGeom& g, int N, const uint32_t* shadow, int words32
 {
     const int G = (N + V - 1) / V;
     const long long need = ((long long)G + kGroupWarps - 1) / kGroupWarps;
-    const long long cap = (long long)sm_count() * 4;
+    const long long cap = (long long)sm_count() * 8;
     const int grid = (int)(need < cap ? need : cap);
     k_reflect_group<Q, V><<<grid, kGroupWarps * 32, 0, st>>>(g.geo_n, N, shadow, words32, table, j0, slab,
                                                               gl.offsets, gl.cells, gl.weights, order, acc);
@@ -410,14 +419,37 @@ cudaError_t group_q(const DevGeom& g, int N, const uint32_t* shadow, int words32
 
 int group_count(int N, int V) { return (N + V - 1) / V; }
 
-cudaError_t launch_group_build(int pass, int V, const DevGeom& g, int N, int T, const NeighborLists& nl,
-                               const int* order, int* counts, const long long* offsets, int* cell,
-                               float* w, int* err, cudaStream_t st)
+cudaError_t launch_weight_lists(int pass, const DevGeom& g, int N, int T, const NeighborLists& nl,
+                                const int* order, int* counts, const long long* woff, int* cells,
+                                float* wts, int* err, cudaStream_t st)
 {
     if (N <= 0) return cudaSuccess;
-    if (V == 4) return build_v<4>(pass, g, N, T, nl, order, counts, offsets, cell, w, err, st);
-    if (V == 8) return build_v<8>(pass, g, N, T, nl, order, counts, offsets, cell, w, err, st);
-    return cudaErrorInvalidValue;
+    const long long threads = (long long)N * 32;
+    const unsigned grid = (unsigned)((threads + 255) / 256);
+    if (nl.format == 0) {
+        if (pass == 0) k_wlist<0, 0><<<grid, 256, 0, st>>>(g.geo_n, g.geo_p, N, T, nl, order, counts, woff, cells, wts, err);
+        else k_wlist<0, 1><<<grid, 256, 0, st>>>(g.geo_n, g.geo_p, N, T, nl, order, counts, woff, cells, wts, err);
+    } else {
+        if (pass == 0) k_wlist<1, 0><<<grid, 256, 0, st>>>(g.geo_n, g.geo_p, N, T, nl, order, counts, woff, cells, wts, err);
+        else k_wlist<1, 1><<<grid, 256, 0, st>>>(g.geo_n, g.geo_p, N, T, nl, order, counts, woff, cells, wts, err);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_merge(int pass, int V, int N, const long long* woff, const int* wcell,
+                               const float* wts, int* counts, const long long* goff, int* cell, float* w,
+                               cudaStream_t st)
+{
+    if (N <= 0) return cudaSuccess;
+    switch (V) {
+    case 2: return pass == 0 ? merge_pass<2, 0>(N, woff, wcell, wts, counts, goff, cell, w, st)
+                             : merge_pass<2, 1>(N, woff, wcell, wts, counts, goff, cell, w, st);
+    case 4: return pass == 0 ? merge_pass<4, 0>(N, woff, wcell, wts, counts, goff, cell, w, st)
+                             : merge_pass<4, 1>(N, woff, wcell, wts, counts, goff, cell, w, st);
+    case 8: return pass == 0 ? merge_pass<8, 0>(N, woff, wcell, wts, counts, goff, cell, w, st)
+                             : merge_pass<8, 1>(N, woff, wcell, wts, counts, goff, cell, w, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_reflect_group(const DevGeom& g, int N, const uint32_t* shadow, int words32,
@@ -439,6 +471,24 @@ cudaError_t launch_reflect_group(const DevGeom& g, int N, const uint32_t* shadow
         case 64: return group_q<2, 4>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
         case 128: return group_q<4, 4>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
         case 256: return group_q<8, 4>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    if (gl.V == 2) {
+        switch (B) {
+        case 64: return group_q<2, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 128: return group_q<4, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 256: return group_q<8, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 512: return group_q<16, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    if (gl.V == 1) {
+        switch (B) {
+        case 64: return group_q<2, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 128: return group_q<4, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 256: return group_q<8, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 512: return group_q<16, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
         default: return cudaErrorInvalidValue;
         }
     }

@@ -82,7 +82,7 @@ struct solar_gpu_context {
         counts, csr_off, csr_ids, barle_off, barle_sizes, barle_bytes, scan_tmp, slab, hourly,
         acc_f64, acc_f32, acc_comp, sums, out_f64, err, in_grid, in_pp, in_wz, in_slopes,
         in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
-        grp_cell, grp_w;
+        grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
@@ -187,16 +187,23 @@ int check_options(const solar_gpu_options* o, bool trace_only)
     if (o->neighbor_format < 0 || o->neighbor_format > 2 || (!trace_only && o->neighbor_format == 2))
         return fail(SOLAR_GPU_ERR_ARG, "neighbor_format %d", o->neighbor_format);
     const int B = o->hour_block;
-    if (!(B == 0 || B == 1 || B == 32 || B == 64 || B == 128 || B == 256))
-        return fail(SOLAR_GPU_ERR_ARG, "hour_block %d (1, 32, 64, 128 or 256)", B);
+    if (!(B == 0 || B == 1 || B == 32 || B == 64 || B == 128 || B == 256 || B == 512))
+        return fail(SOLAR_GPU_ERR_ARG, "hour_block %d (1, 32, 64, 128, 256 or 512)", B);
     if (o->accumulation < 0 || o->accumulation > 2) return fail(SOLAR_GPU_ERR_ARG, "accumulation %d", o->accumulation);
     if (o->reflection < 0 || o->reflection > 1) return fail(SOLAR_GPU_ERR_ARG, "reflection %d", o->reflection);
     if (o->chunk_voxels < 0) return fail(SOLAR_GPU_ERR_ARG, "chunk_voxels %lld", o->chunk_voxels);
-    if (!(o->group_size == 0 || o->group_size == 4 || o->group_size == 8))
-        return fail(SOLAR_GPU_ERR_ARG, "group_size %d (0, 4 or 8)", o->group_size);
+    // hour-block widths each reflection kernel is built for
+    const int V = o->group_size;
     const int Bq = B == 0 ? 128 : B;
-    if (Bq > 1 && ((o->group_size == 8 && Bq > 128) || (o->group_size == 4 && Bq > 256)))
-        return fail(SOLAR_GPU_ERR_ARG, "hour_block %d too wide for group_size %d", Bq, o->group_size);
+    bool ok = false;
+    switch (V) {
+    case 0: case 4: ok = Bq >= 32 && Bq <= 256; break;
+    case 8: ok = Bq >= 32 && Bq <= 128; break;
+    case 1: case 2: ok = Bq >= 64 && Bq <= 512; break;
+    default: return fail(SOLAR_GPU_ERR_ARG, "group_size %d (0, 1, 2, 4 or 8)", V);
+    }
+    if (Bq > 1 && !ok)
+        return fail(SOLAR_GPU_ERR_ARG, "hour_block %d is not built for group_size %d", Bq, V);
     return SOLAR_GPU_OK;
 }
 
@@ -222,7 +229,7 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
     sky = make_sky_tables(s->sun_positions);
     const int D = (int)sky.dirs.size();
     const int Hd = (int)sky.hour_index.size();
-    const int n_padded = ((Hd + 255) / 256) * 256 + 256;
+    const int n_padded = ((Hd + 511) / 512) * 512 + 512;   // room for the widest hour block
     RK(ensure(c->dirs, sizeof(DirEntry) * D));
     RK(ensure(c->nudged, sizeof(float) * 2 * kHoursPerYear));
     RK(ensure(c->dni, sizeof(float) * kHoursPerYear));
@@ -265,11 +272,13 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
         const long long npos = order_positions(s->grid_width, s->grid_height);
         RK(ensure(c->order, sizeof(int) * (size_t)N));
         RK(ensure(c->order_cnt, sizeof(int) * (size_t)npos));
+        RK(ensure(c->order_first, sizeof(int) * ((size_t)npos + 1)));
         RK(ensure(c->order_cur, sizeof(long long) * ((size_t)npos + 1)));
         RK(ensure(c->order_tmp, sizeof(long long) * scan_scratch_elems((int)npos)));
         KScope k(c, SOLAR_GPU_KT_SETUP);
-        CK(launch_voxel_order(s->pixel_parent, N, s->grid_width, s->grid_height, as<int>(c->order_cnt),
-                              as<long long>(c->order_cur), as<long long>(c->order_tmp), as<int>(c->order), st));
+        CK(launch_voxel_order(s->pixel_parent, N, s->num_top_voxels, s->grid_width, s->grid_height,
+                              as<int>(c->order_cnt), as<int>(c->order_first), as<long long>(c->order_cur),
+                              as<long long>(c->order_tmp), as<int>(c->order), st));
     }
     c->launches += 8;
     return SOLAR_GPU_OK;
@@ -445,34 +454,62 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         float* slab = as<float>(c->slab);
         GroupLists gl{o->group_size, nullptr, nullptr, nullptr};
         if (o->group_size > 0) {
-            // merged weighted union lists of each group of V voxels (once per run)
+            // Once per run: the nonzero weights of every list in visiting order,
+            // then (V > 1) the merged union entries of each group of V voxels.
             const int V = o->group_size;
-            const int G = group_count(N, V);
-            RK(ensure(c->grp_cnt, sizeof(int) * (size_t)G));
-            RK(ensure(c->grp_off, sizeof(long long) * ((size_t)G + 1)));
-            RK(ensure(c->grp_tmp, sizeof(long long) * scan_scratch_elems(G)));
+            RK(ensure(c->w_cnt, sizeof(int) * (size_t)N));
+            RK(ensure(c->w_off, sizeof(long long) * ((size_t)N + 1)));
+            RK(ensure(c->w_tmp, sizeof(long long) * scan_scratch_elems(N)));
             {
                 KScope k(c, SOLAR_GPU_KT_GROUP);
-                CK(launch_group_build(0, V, g, N, T, nl, as<int>(c->order), as<int>(c->grp_cnt), nullptr,
-                                      nullptr, nullptr, err, st));
-                CK(launch_scan_counts(as<int>(c->grp_cnt), G, 0, as<long long>(c->grp_off),
-                                      as<long long>(c->grp_tmp), nullptr, st));
+                CK(launch_weight_lists(0, g, N, T, nl, as<int>(c->order), as<int>(c->w_cnt), nullptr, nullptr,
+                                       nullptr, err, st));
+                CK(launch_scan_counts(as<int>(c->w_cnt), N, 0, as<long long>(c->w_off), as<long long>(c->w_tmp),
+                                      nullptr, st));
             }
-            long long E = 0;
-            RK(read_ll(c, as<long long>(c->grp_off) + G, &E, st));
-            RK(ensure(c->grp_cell, sizeof(int) * (size_t)(E + 1)));
-            RK(ensure(c->grp_w, sizeof(float) * (size_t)(E + 1) * V));
+            long long Ew = 0;
+            RK(read_ll(c, as<long long>(c->w_off) + N, &Ew, st));
+            RK(ensure(c->w_cell, sizeof(int) * (size_t)(Ew + 1)));
+            RK(ensure(c->w_val, sizeof(float) * (size_t)(Ew + 1)));
             {
                 KScope k(c, SOLAR_GPU_KT_GROUP);
-                CK(launch_group_build(1, V, g, N, T, nl, as<int>(c->order), as<int>(c->grp_cnt),
-                                      as<long long>(c->grp_off), as<int>(c->grp_cell), as<float>(c->grp_w),
-                                      err, st));
+                CK(launch_weight_lists(1, g, N, T, nl, as<int>(c->order), nullptr, as<long long>(c->w_off),
+                                       as<int>(c->w_cell), as<float>(c->w_val), err, st));
             }
-            c->group_entries = E;
             c->launches += 5;
-            gl.offsets = as<long long>(c->grp_off);
-            gl.cells = as<int>(c->grp_cell);
-            gl.weights = as<float>(c->grp_w);
+            if (V == 1) {
+                c->group_entries = Ew;
+                gl.offsets = as<long long>(c->w_off);
+                gl.cells = as<int>(c->w_cell);
+                gl.weights = as<float>(c->w_val);
+            } else {
+                const int G = group_count(N, V);
+                RK(ensure(c->grp_cnt, sizeof(int) * (size_t)G));
+                RK(ensure(c->grp_off, sizeof(long long) * ((size_t)G + 1)));
+                RK(ensure(c->grp_tmp, sizeof(long long) * scan_scratch_elems(G)));
+                {
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(launch_group_merge(0, V, N, as<long long>(c->w_off), as<int>(c->w_cell), as<float>(c->w_val),
+                                          as<int>(c->grp_cnt), nullptr, nullptr, nullptr, st));
+                    CK(launch_scan_counts(as<int>(c->grp_cnt), G, 0, as<long long>(c->grp_off),
+                                          as<long long>(c->grp_tmp), nullptr, st));
+                }
+                long long E = 0;
+                RK(read_ll(c, as<long long>(c->grp_off) + G, &E, st));
+                RK(ensure(c->grp_cell, sizeof(int) * (size_t)(E + 1)));
+                RK(ensure(c->grp_w, sizeof(float) * (size_t)(E + 1) * V));
+                {
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(launch_group_merge(1, V, N, as<long long>(c->w_off), as<int>(c->w_cell), as<float>(c->w_val),
+                                          as<int>(c->grp_cnt), as<long long>(c->grp_off), as<int>(c->grp_cell),
+                                          as<float>(c->grp_w), st));
+                }
+                c->group_entries = E;
+                c->launches += 5;
+                gl.offsets = as<long long>(c->grp_off);
+                gl.cells = as<int>(c->grp_cell);
+                gl.weights = as<float>(c->grp_w);
+            }
         }
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
@@ -633,7 +670,8 @@ void solar_gpu_destroy(solar_gpu_context* c)
                       &c->acc_f64, &c->acc_f32, &c->acc_comp, &c->sums, &c->out_f64, &c->err, &c->in_grid,
                       &c->in_pp, &c->in_wz, &c->in_slopes, &c->in_aspects, &c->out_f32, &c->order,
                       &c->order_cnt, &c->order_cur, &c->order_tmp, &c->grp_cnt, &c->grp_off,
-                      &c->grp_tmp, &c->grp_cell, &c->grp_w};
+                      &c->grp_tmp, &c->grp_cell, &c->grp_w, &c->w_cnt, &c->w_off, &c->w_tmp,
+                      &c->w_cell, &c->w_val, &c->order_first};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (cudaEvent_t e : c->kt_pool) cudaEventDestroy(e);

@@ -464,17 +464,40 @@ __device__ __forceinline__ long long cell_pos(int c, int W, int ntx)
     return (tile << (2 * kTileBits)) | (spread5((unsigned)x) | (spread5((unsigned)y) << 1));
 }
 
-__global__ void k_order_count(const int* __restrict__ pp, int N, int W, int ntx, int* __restrict__ cnt)
+__global__ void k_order_count(const int* __restrict__ pp, int N, int T, int W, int ntx, int* __restrict__ cnt,
+                              int* __restrict__ first_wall)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < N) atomicAdd(cnt + cell_pos(pp[v], W, ntx), 1);
+    if (v >= N) return;
+    const long long pos = cell_pos(pp[v], W, ntx);
+    atomicAdd(cnt + pos, 1);
+    if (v >= T) atomicMin(first_wall + pos, v);
 }
 
-__global__ void k_order_scatter(const int* __restrict__ pp, int N, int W, int ntx,
-                                unsigned long long* __restrict__ cursor, int* __restrict__ order)
+// Deterministic placement: the top voxel first, then the cell's walls in
+// index order (they are contiguous by the voxel layout of src/main.cpp:112-127).
+// A cell whose walls are not contiguous sets *flag and the fallback below
+// places every voxel with atomic cursors instead (correct, order within a
+// cell then arbitrary).
+__global__ void k_order_scatter(const int* __restrict__ pp, int N, int T, int W, int ntx,
+                                const int* __restrict__ cnt, const long long* __restrict__ base,
+                                const int* __restrict__ first_wall, int* __restrict__ order, int* __restrict__ flag)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < N) order[atomicAdd(cursor + cell_pos(pp[v], W, ntx), 1ull)] = v;
+    if (v >= N) return;
+    const long long pos = cell_pos(pp[v], W, ntx);
+    const long long rank = v < T ? 0 : 1 + (long long)v - first_wall[pos];
+    if (rank < cnt[pos]) order[base[pos] + rank] = v;
+    else atomicOr(flag, 1);
+}
+
+__global__ void k_order_scatter_fallback(const int* __restrict__ pp, int N, int W, int ntx,
+                                         unsigned long long* __restrict__ cursor, int* __restrict__ order,
+                                         const int* __restrict__ flag)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N || *flag == 0) return;
+    order[atomicAdd(cursor + cell_pos(pp[v], W, ntx), 1ull)] = v;
 }
 }  // namespace
 
@@ -485,19 +508,26 @@ long long order_positions(int W, int H)
     return ntx * nty << (2 * kTileBits);
 }
 
-cudaError_t launch_voxel_order(const int* pix_parent, int N, int W, int H, int* counts,
-                               long long* cursor, long long* scan_tmp, int* order, cudaStream_t st)
+cudaError_t launch_voxel_order(const int* pix_parent, int N, int T, int W, int H, int* counts,
+                               int* first_wall, long long* cursor, long long* scan_tmp, int* order,
+                               cudaStream_t st)
 {
     if (N <= 0) return cudaSuccess;
     const int ntx = (W + (1 << kTileBits) - 1) >> kTileBits;
     const long long npos = order_positions(W, H);
+    int* flag = first_wall + npos;
     cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * npos, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(first_wall, 0x7F, sizeof(int) * npos, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    k_order_count<<<(N + 255) / 256, 256, 0, st>>>(pix_parent, N, W, ntx, counts);
+    k_order_count<<<(N + 255) / 256, 256, 0, st>>>(pix_parent, N, T, W, ntx, counts, first_wall);
     e = launch_scan_counts(counts, (int)npos, 0, cursor, scan_tmp, nullptr, st);
     if (e != cudaSuccess) return e;
-    k_order_scatter<<<(N + 255) / 256, 256, 0, st>>>(pix_parent, N, W, ntx,
-                                                    reinterpret_cast<unsigned long long*>(cursor), order);
+    k_order_scatter<<<(N + 255) / 256, 256, 0, st>>>(pix_parent, N, T, W, ntx, counts, cursor, first_wall,
+                                                    order, flag);
+    k_order_scatter_fallback<<<(N + 255) / 256, 256, 0, st>>>(pix_parent, N, W, ntx,
+                                                             reinterpret_cast<unsigned long long*>(cursor),
+                                                             order, flag);
     return cudaGetLastError();
 }
 

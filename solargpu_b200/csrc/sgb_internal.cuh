@@ -113,8 +113,9 @@ cudaError_t launch_reflect_block(const DevGeom& g, int N, int T, const uint32_t*
                                  const int* order, int* err, cudaStream_t st);
 // Visiting order of the reflection pass (32 x 32 cell tiles, Morton inside).
 long long order_positions(int W, int H);
-cudaError_t launch_voxel_order(const int* pix_parent, int N, int W, int H, int* counts,
-                               long long* cursor, long long* scan_tmp, int* order, cudaStream_t st);
+cudaError_t launch_voxel_order(const int* pix_parent, int N, int T, int W, int H, int* counts,
+                               int* first_wall, long long* cursor, long long* scan_tmp, int* order,
+                               cudaStream_t st);
 cudaError_t launch_reflect_hour(const DevGeom& g, int N, int T, const float* hourly,
                                 const NeighborLists& nl, const Accum& acc, int* err,
                                 cudaStream_t st);
@@ -125,15 +126,21 @@ cudaError_t launch_finalize(const Accum& acc, int N, float* out, cudaStream_t st
 
 // grouped reflection (group.cu)
 struct GroupLists {
-    int V;                       // voxels per group (4 or 8)
+    int V;                       // voxels per group (1, 2, 4 or 8)
     const long long* offsets;    // [G + 1] union entries per group
     const int* cells;            // [E] neighbor cell of each union entry, ascending per group
     const float* weights;        // [E][V] weight of that cell for each voxel of the group
 };
 int group_count(int N, int V);
-cudaError_t launch_group_build(int pass, int V, const DevGeom& g, int N, int T, const NeighborLists& nl,
-                               const int* order, int* counts, const long long* offsets, int* cell,
-                               float* w, int* err, cudaStream_t st);
+// Weighted lists in visiting order: pass 0 counts nonzero weights per
+// position, pass 1 writes (cell, w) at woff[p].
+cudaError_t launch_weight_lists(int pass, const DevGeom& g, int N, int T, const NeighborLists& nl,
+                                const int* order, int* counts, const long long* woff, int* cells,
+                                float* wts, int* err, cudaStream_t st);
+// Merges the weighted lists of V consecutive positions into union entries.
+cudaError_t launch_group_merge(int pass, int V, int N, const long long* woff, const int* wcell,
+                               const float* wts, int* counts, const long long* goff, int* cell, float* w,
+                               cudaStream_t st);
 cudaError_t launch_reflect_group(const DevGeom& g, int N, const uint32_t* shadow, int words32,
                                  const HourEntry* table, int j0, int B, const float* slab,
                                  const GroupLists& gl, const int* order, const Accum& acc, cudaStream_t st);

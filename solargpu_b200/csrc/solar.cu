@@ -90,19 +90,33 @@ __global__ void k_voxel_geom(DevScene s, float4* __restrict__ geo_n, float4* __r
     geo_p[v] = make_float4((float)gx, (float)gy, z, 0.0f);
 }
 
-// slab[g * B + b] = I(g, j0 + b) for every top cell g.
+// slab[g * B + b] = I(g, j0 + b) for every top cell g.  A warp owns 32
+// consecutive hours of the block (their table entries stay in registers)
+// and sweeps a run of cells, writing one coalesced 128-byte row piece per
+// cell; the voxel normal is a broadcast load.
+constexpr int kSlabCellsPerWarp = 64;
+
 __global__ void __launch_bounds__(256)
 k_solar_slab(const float4* __restrict__ geo_n, int T, const uint32_t* __restrict__ shadow, int words32,
-             const HourEntry* __restrict__ table, int j0, int log2B, float* __restrict__ slab)
+             const HourEntry* __restrict__ table, int j0, int B, float* __restrict__ slab)
 {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long total = (long long)T << log2B;
-    if (idx >= total) return;
-    const int g = (int)(idx >> log2B);
-    const int b = (int)(idx & ((1 << log2B) - 1));
+    const int lane = threadIdx.x & 31;
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int hchunks = B >> 5;
+    const int hc = (int)(wid % hchunks);
+    const long long g0 = (wid / hchunks) * kSlabCellsPerWarp;
+    if (g0 >= T) return;
+    const int b = hc * 32 + lane;
     const HourEntry e = table[j0 + b];
-    const float4 n4 = __ldg(geo_n + g);
-    slab[idx] = solar_I(n4, e, shadow_bit(shadow, words32, g, e.dense));
+    const int word = e.dense >= 0 ? (e.dense >> 5) : 0;
+    const uint32_t mask = e.dense >= 0 ? (1u << (e.dense & 31)) : 0u;
+    const long long g1 = min((long long)T, g0 + kSlabCellsPerWarp);
+#pragma unroll 4
+    for (long long g = g0; g < g1; ++g) {
+        const float4 n4 = __ldg(geo_n + g);
+        const uint32_t bit = (__ldg(shadow + g * words32 + word) & mask) ? 1u : 0u;
+        slab[g * B + b] = solar_I(n4, e, bit);
+    }
 }
 
 __global__ void __launch_bounds__(256)
@@ -154,12 +168,10 @@ cudaError_t launch_voxel_geom(const DevScene& s, DevGeom g, cudaStream_t st)
 cudaError_t launch_solar_slab(const DevGeom& g, int T, const uint32_t* shadow, int words32,
                               const HourEntry* table, int j0, int B, float* slab, cudaStream_t st)
 {
-    int log2B = 0;
-    while ((1 << log2B) < B) ++log2B;
-    if ((1 << log2B) != B) return cudaErrorInvalidValue;
-    const long long total = (long long)T << log2B;
-    k_solar_slab<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(g.geo_n, T, shadow, words32, table,
-                                                                  j0, log2B, slab);
+    if (B < 32 || (B & 31)) return cudaErrorInvalidValue;
+    const long long warps = ((long long)T + kSlabCellsPerWarp - 1) / kSlabCellsPerWarp * (B / 32);
+    k_solar_slab<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(g.geo_n, T, shadow, words32, table,
+                                                                        j0, B, slab);
     return cudaGetLastError();
 }
 

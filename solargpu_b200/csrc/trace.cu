@@ -26,6 +26,7 @@ namespace {
 constexpr int kTraceBlock = 128;
 constexpr int kDedupeWarps = 4;
 constexpr int kHashSlots = 4096;   // > 2592 possible distinct hits per voxel
+constexpr int kDedupeBatch = 9;    // 2592 = 9 batches of 9 rounds of 32 directions
 
 __device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, int H, float maxz,
                                          int gx, int gy, float base_z, const DirEntry& d)
@@ -122,27 +123,37 @@ k_dedupe(int chunk_count, int D, int* __restrict__ raw, int* __restrict__ counts
     __syncwarp();
     int* row = raw + (size_t)lv * D;
     int n = 0;
-    for (int base = 0; base < D; base += 32) {
-        const int d = base + lane;
-        const int h = (d < D) ? row[d] : 0;
-        const unsigned same = __match_any_sync(0xFFFFFFFFu, h);
-        const bool leader = (__ffs(same) - 1) == lane;
-        bool fresh = false;
-        if (h != 0 && leader) {
-            uint32_t slot = hash_slot((uint32_t)h);
-            int probe = 0;
-            for (; probe < kHashSlots; ++probe) {
-                const uint32_t old = atomicCAS(&tab[slot], 0u, (uint32_t)h);
-                if (old == 0u) { fresh = true; break; }
-                if (old == (uint32_t)h) break;
-                slot = (slot + 1) & (kHashSlots - 1);
-            }
-            if (probe == kHashSlots) atomicOr(err, kErrHashFull);
+    // Rounds of 32 directions, kDedupeBatch rounds loaded ahead (they are
+    // all read before any in-place write can reach their slots).
+    for (int base = 0; base < D; base += 32 * kDedupeBatch) {
+        int hv[kDedupeBatch];
+#pragma unroll
+        for (int u = 0; u < kDedupeBatch; ++u) {
+            const int d = base + 32 * u + lane;
+            hv[u] = (d < D) ? row[d] : 0;
         }
-        const unsigned bal = __ballot_sync(0xFFFFFFFFu, fresh);
-        // Writes land below base + 32: every slot there was read this round.
-        if (fresh) row[n + __popc(bal & ((1u << lane) - 1u))] = h;
-        n += __popc(bal);
+#pragma unroll
+        for (int u = 0; u < kDedupeBatch; ++u) {
+            const int h = hv[u];
+            const unsigned same = __match_any_sync(0xFFFFFFFFu, h);
+            const bool leader = (__ffs(same) - 1) == lane;
+            bool fresh = false;
+            if (h != 0 && leader) {
+                uint32_t slot = hash_slot((uint32_t)h);
+                int probe = 0;
+                for (; probe < kHashSlots; ++probe) {
+                    const uint32_t old = atomicCAS(&tab[slot], 0u, (uint32_t)h);
+                    if (old == 0u) { fresh = true; break; }
+                    if (old == (uint32_t)h) break;
+                    slot = (slot + 1) & (kHashSlots - 1);
+                }
+                if (probe == kHashSlots) atomicOr(err, kErrHashFull);
+            }
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, fresh);
+            // Writes land below base + 32 * (u + 1): every slot there was read.
+            if (fresh) row[n + __popc(bal & ((1u << lane) - 1u))] = h;
+            n += __popc(bal);
+        }
     }
     if (lane == 0) counts[lv] = n;
 }

@@ -75,7 +75,8 @@ def test_trace_matches_reference_kernel(ctx, scene64):
 CASES = ([(fmt, 1, acc, 0) for fmt in (0, 1) for acc in (0, 1, 2)]
          + [(fmt, B, acc, 0) for fmt in (0, 1) for B in (32, 64, 128, 256) for acc in (0, 1, 2)]
          + [(fmt, B, acc, V) for fmt in (0, 1) for V in (4, 8) for B in (32, 64, 128, 256) for acc in (0, 1, 2)
-            if not (V == 8 and B == 256)])
+            if not (V == 8 and B == 256)]
+         + [(fmt, B, acc, V) for fmt in (0, 1) for V in (1, 2) for B in (64, 128, 256, 512) for acc in (0, 1)])
 
 
 @pytest.mark.parametrize("fmt,B,acc,V", CASES)
@@ -102,7 +103,7 @@ def test_annual_form_vs_fp64(ctx, scene160, fmt):
     assert e.max() <= REL_TOL, (e.max(), e.mean())
 
 
-@pytest.mark.parametrize("fmt,V", [(0, 0), (1, 0), (0, 8), (1, 8), (1, 4)])
+@pytest.mark.parametrize("fmt,V", [(0, 0), (1, 0), (0, 8), (1, 8), (1, 4), (0, 1), (1, 2)])
 def test_hour_block_vs_fp64_dsm160(ctx, scene160, fmt, V):
     import torch
     s = scene160
