@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--format", type=int, default=1, help="0 = CSR, 1 = ba-RLE")
     ap.add_argument("--hour-block", type=int, default=256)
     ap.add_argument("--accumulation", type=int, default=1)
+    ap.add_argument("--group-size", type=int, default=1)
+    ap.add_argument("--ref-workload", default="dsm256",
+                    help="reference arm: workload timed per step (a full reference run of dsm1024 takes ~6 min)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-hour comparison run")
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 error check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -155,16 +158,22 @@ def workload_desc(scene, name: str) -> str:
             f"lat {c.lat} lon {c.lon} tz +{c.tz}, synthetic TMY")
 
 
-def roofline_bytes(scene, ctx_sizes, fmt, B, acc) -> float:
-    """Algorithmic HBM bytes of one hour-block reflection launch (gathered slab
-    rows counted once, as cache hits): neighbor stream + offsets + geometry +
-    shadow words + accumulator read/write per voxel, plus one read of the
-    block's top-cell slab."""
+def roofline_bytes(scene, ctx_sizes, fmt, B, acc, V, entries) -> float:
+    """Algorithmic HBM bytes of one hour-block reflection launch, gathered
+    slab rows counted once (as cache hits): the streamed lists (V = 0: CSR ids
+    or ba-RLE bytes + offsets; V >= 1: entries of one cell id + V weights +
+    group offsets), per voxel the visiting-order index, geometry, shadow words
+    and accumulator read/write, plus one read of the block's top-cell slab."""
     csr_entries, barle_bytes, words32 = ctx_sizes
     N, T = scene.num_total, scene.num_top
-    lists = barle_bytes if fmt == 1 else 4 * csr_entries
     acc_b = 16 if acc in (0, 1) else 8
-    return float(lists + N * (8 + 32 + 4 * words32 + acc_b) + T * B * 4)
+    if V == 0:
+        lists = (barle_bytes if fmt == 1 else 4 * csr_entries) + 8 * (N + 1)
+        per_voxel = 4 + 32 + 4 * words32 + acc_b
+    else:
+        lists = entries * (4 + 4 * V) + 8 * (N // V + 2)
+        per_voxel = 4 + 16 + 4 * words32 + acc_b
+    return float(lists + N * per_voxel + T * B * 4)
 
 
 # ---------------------------------------------------------------- our arm
@@ -189,7 +198,7 @@ def run_ours(args, world, rank, local, pg):
     stream = torch.cuda.current_stream(dev)
     ctx = api.Context(local)
     opts = dict(neighbor_format=args.format, hour_block=args.hour_block, accumulation=args.accumulation,
-                use_graph=0, time_kernels=1)
+                group_size=args.group_size, use_graph=0, time_kernels=1)
 
     def step():
         ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
@@ -244,11 +253,16 @@ def run_ours(args, world, rank, local, pg):
     dom = max(ktimes.items(), key=lambda kv: kv[1][0])
     refl_ms, refl_n = ktimes.get("reflect", (0.0, 0))
     B = args.hour_block
-    alg = roofline_bytes(scene, (ne.value, nb.value, w.value), args.format, B, args.accumulation)
+    V = args.group_size
+    entries = ctx.reflection_entries()
+    alg = roofline_bytes(scene, (ne.value, nb.value, w.value), args.format, B, args.accumulation, V, entries)
     per_launch_ms = refl_ms / max(1, refl_n)
     achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    # slab values moved through L1 per launch (one row of B floats per entry)
+    gathered = float(entries if V >= 1 else ne.value) * B * 4
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"reflect_block_{args.workload}_{FMT_NAMES[args.format].replace('-', '').lower()}_b{B}.md")
+    kname = "reflect_group" if V >= 1 else "reflect_block"
+    prof = os.path.join(ROOT, "profiles", f"{kname}_{args.workload}_{FMT_NAMES[args.format].replace('-', '').lower()}_b{B}_v{V}.md")
     if os.path.exists(prof):
         for ln in open(prof):
             if ln.strip().startswith("traffic_bytes_per_launch:"):
@@ -256,12 +270,16 @@ def run_ours(args, world, rank, local, pg):
                     traffic = float(ln.split(":", 1)[1].split()[0])
                 except ValueError:
                     pass
-    roof = {"bound": "hbm", "kernel": "k_reflect_block (hour-block SpMM + accumulation)",
+    kdesc = (f"k_reflect_group<{B // 32},{V}> (hour-block sparse x dense product over weighted lists + accumulation)"
+             if V >= 1 else f"k_reflect_block<{B // 32},{args.format}> (hour-block sparse x dense product + accumulation)")
+    roof = {"bound": "hbm", "kernel": kdesc,
             "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 5), "peak_source": peak_src,
             "traffic": traffic, "alg_bytes_per_launch": alg, "launch_ms": round(per_launch_ms, 4),
             "share_of_step": round(refl_ms / max(1e-9, sum(v[0] for v in ktimes.values())), 4),
-            "dominant_group": dom[0]}
+            "dominant_group": dom[0],
+            "gathered_slab_bytes_per_launch": gathered,
+            "l1_gather_gbs": round(gathered / (per_launch_ms / 1e3) / 1e9, 1) if per_launch_ms > 0 else None}
 
     # ---- end to end through the host API (pinned host buffers in and out)
     e2e = None
@@ -271,7 +289,8 @@ def run_ours(args, world, rank, local, pg):
                           pinned_copy(scene.sun), pinned_copy(scene.direct), pinned_copy(scene.diffuse),
                           pinned_copy(scene.slopes), pinned_copy(scene.aspects))
         hout = pinned_copy(np.zeros(N, np.float32))
-        eopts = dict(neighbor_format=args.format, hour_block=B, accumulation=args.accumulation, use_graph=1)
+        eopts = dict(neighbor_format=args.format, hour_block=B, accumulation=args.accumulation,
+                     group_size=args.group_size, use_graph=1)
         ctx.run_host(hs, hout, **eopts)
         barrier(pg)
         wall = []
@@ -301,6 +320,26 @@ def run_ours(args, world, rank, local, pg):
         extra["plain_per_hour"] = {"ms_per_step": round(plain_ms, 2), "value": units / (plain_ms / 1e3),
                                    "speedup": round(plain_ms / ms_per_step, 2),
                                    "config": "hour_block 1 (one solar + one reflection launch per daylight hour), plain fp32"}
+        ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
+        torch.cuda.synchronize(dev)
+    if rank == 0:
+        # the other neighbor-list format on the same workload (both paths run here)
+        ofmt = 1 - args.format
+        oopts = dict(opts, neighbor_format=ofmt, time_kernels=0)
+        ctx.run_device(scene, d, out, stream=stream.cuda_stream, **oopts)
+        oms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.run_device(scene, d, out, stream=stream.cuda_stream, **oopts)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            oms.append(e0.elapsed_time(e1))
+        extra[f"{FMT_NAMES[ofmt].replace('-', '').lower()}_path"] = {
+            "ms_per_step": round(sum(oms) / len(oms), 2), "value": units / (sum(oms) / len(oms) / 1e3),
+            "neighbor_format": FMT_NAMES[ofmt]}
         ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
         torch.cuda.synchronize(dev)
     if rank == 0 and not args.no_check:
@@ -369,11 +408,14 @@ def run_reference(args, world, rank, local, pg):
     if O.ref_gpu() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsolarref.so was not built"}))
         return
-    scene = inputs.make_scene(args.workload)
+    # A full reference run of the 1024 x 1024 city takes about 6 minutes, so
+    # each step times the reference on a bounded sample: the same generator at
+    # 256 x 256 (same building/tree densities), one full annual run per step.
+    scene = inputs.make_scene(args.ref_workload)
     comp = args.format == 1
     Hd = int(((scene.sun[:, 1] - np.float32(1e-8)) >= 1.0).sum())
     units = float(scene.num_total) * Hd
-    for _ in range(args.warmup):
+    for _ in range(min(args.warmup, 1)):
         with quiet_stdout():
             O.ref_irradiance(scene, comp)
     wall = []
@@ -386,13 +428,14 @@ def run_reference(args, world, rank, local, pg):
     value = units * args.steps / sec
     desc = ("reference CUDA pipeline (src/cuda/*.cu, sm_100a build of the unmodified sources) through its stock "
             f"API solar_gpu::{'compressed' if comp else 'uncompressed'}_gpu_irradiance, host buffers in/out; "
-            "one full annual run per step")
+            f"one full annual run of {args.ref_workload} per step (bounded sample of {args.workload})")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": workload_desc(scene, args.workload), "voxels": scene.num_total,
-                       "daylight_hours": Hd, "neighbor_format": FMT_NAMES[args.format]},
+            "config": {"workload": workload_desc(scene, args.ref_workload), "voxels": scene.num_total,
+                       "daylight_hours": Hd, "neighbor_format": FMT_NAMES[args.format],
+                       "sample_of": args.workload, "warmup_runs": min(args.warmup, 1)},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": desc + " (the reference has no CPU path; its host thread drives the GPU)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

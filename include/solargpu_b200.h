@@ -171,6 +171,10 @@ enum {
 };
 int solar_gpu_kernel_times(solar_gpu_context* ctx, double* ms, long long* launches, int n);
 
+/* Entries the hour-block reflection streamed per block in the last run
+   (weighted or merged union entries; 0 for group_size 0). */
+long long solar_gpu_last_reflection_entries(solar_gpu_context* ctx);
+
 /* Number of kernel launches the library issued in the last run. */
 long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
 

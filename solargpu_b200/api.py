@@ -66,6 +66,8 @@ def lib() -> C.CDLL:
         L.solar_gpu_last_error.restype = C.c_char_p
         L.solar_gpu_last_launch_count.restype = ll
         L.solar_gpu_last_launch_count.argtypes = [vp]
+        L.solar_gpu_last_reflection_entries.restype = ll
+        L.solar_gpu_last_reflection_entries.argtypes = [vp]
         for name in ("solar_gpu_uncompressed_gpu_irradiance", "solar_gpu_compressed_gpu_irradiance"):
             fn = getattr(L, name)
             fn.argtypes = [vp, i, i, i, i, vp, vp, f, vp, i, vp, i, vp, i, vp, vp, vp]
@@ -271,6 +273,10 @@ class Context:
         if n < 0:
             _check(n)
         return {g: (ms[i], int(ln[i])) for i, g in enumerate(self.KERNEL_GROUPS[:n])}
+
+    def reflection_entries(self) -> int:
+        """Weighted/union entries streamed per hour block in the last run."""
+        return int(lib().solar_gpu_last_reflection_entries(self.h))
 
     def launches(self) -> int:
         return int(lib().solar_gpu_last_launch_count(self.h))

@@ -148,18 +148,19 @@ __device__ int load_sorted(const int* row, int k, uint32_t* ids, int lane, bool 
 template <int IDS, int RUNS, int WARPS, bool LARGE>
 __global__ void __launch_bounds__(WARPS * 32)
 k_barle_size(int chunk_count, int D, int* __restrict__ raw, const int* __restrict__ counts,
-             int* __restrict__ sizes, int* __restrict__ err)
+             int* __restrict__ sizes, int* __restrict__ err, const int* __restrict__ perm)
 {
     extern __shared__ uint32_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t* ids = smem + warp * (IDS + RUNS);
     uint32_t* runs = ids + IDS;
-    const int lv = blockIdx.x * WARPS + warp;
+    const int lv = blockIdx.x * WARPS + warp;   // row
     if (lv >= chunk_count) return;
-    const int k = counts[lv];
+    const int u = perm ? perm[lv] : lv;          // voxel of the row
+    const int k = counts[u];
     if (LARGE != (k > kSmallIds)) return;
-    if (k <= 0) { if (lane == 0) sizes[lv] = 0; return; }
-    if (k > D || k > RUNS) { if (lane == 0) { sizes[lv] = 0; atomicOr(err, kErrListCapacity); } return; }
+    if (k <= 0) { if (lane == 0) sizes[u] = 0; return; }
+    if (k > D || k > RUNS) { if (lane == 0) { sizes[u] = 0; atomicOr(err, kErrListCapacity); } return; }
     int* row = raw + (size_t)lv * D;
     load_sorted(row, k, ids, lane, true);
     for (int i = lane; i < k; i += 32) row[i] = (int)ids[i];   // keep the sorted list for the write pass
@@ -176,14 +177,14 @@ k_barle_size(int chunk_count, int D, int* __restrict__ raw, const int* __restric
         pieces += __shfl_xor_sync(0xFFFFFFFFu, pieces, o);
         payload += __shfl_xor_sync(0xFFFFFFFFu, payload, o);
     }
-    if (lane == 0) sizes[lv] = 3 * ((pieces + 7) / 8) + pieces + payload;
+    if (lane == 0) sizes[u] = 3 * ((pieces + 7) / 8) + pieces + payload;
 }
 
 template <int IDS, int RUNS, int WARPS, bool LARGE>
 __global__ void __launch_bounds__(WARPS * 32)
 k_barle_write(int chunk_count, int D, const int* __restrict__ raw, const int* __restrict__ counts,
               const long long* __restrict__ offsets, unsigned char* __restrict__ out,
-              int* __restrict__ err)
+              int* __restrict__ err, const int* __restrict__ inv)
 {
     extern __shared__ uint32_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -194,7 +195,7 @@ k_barle_write(int chunk_count, int D, const int* __restrict__ raw, const int* __
     const int k = counts[lv];
     if (LARGE != (k > kSmallIds)) return;
     if (k <= 0 || k > D || k > RUNS) return;
-    const int* row = raw + (size_t)lv * D;
+    const int* row = raw + (size_t)(inv ? inv[lv] : lv) * D;
     load_sorted(row, k, ids, lane, false);   // already sorted by k_barle_size
     int nr = build_runs(ids, k, runs, lane);
     // split_long_runs (barle_compression.cpp:29-44), expanded in place from the back
@@ -262,48 +263,63 @@ k_barle_write(int chunk_count, int D, const int* __restrict__ raw, const int* __
 }  // namespace
 
 template <int IDS, int RUNS, int WARPS, bool LARGE>
-cudaError_t size_pass(int chunk_count, int D, int* raw, const int* counts, int* sizes, int* err, cudaStream_t st)
+cudaError_t size_pass(int chunk_count, int D, int* raw, const int* counts, int* sizes, int* err, const int* perm,
+                      cudaStream_t st)
 {
     const size_t smem = (size_t)WARPS * (IDS + RUNS) * sizeof(uint32_t);
     cudaError_t e = cudaFuncSetAttribute(k_barle_size<IDS, RUNS, WARPS, LARGE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_barle_size<IDS, RUNS, WARPS, LARGE><<<(chunk_count + WARPS - 1) / WARPS, WARPS * 32, smem, st>>>(
-        chunk_count, D, raw, counts, sizes, err);
+        chunk_count, D, raw, counts, sizes, err, perm);
     return cudaGetLastError();
 }
 
 template <int IDS, int RUNS, int WARPS, bool LARGE>
 cudaError_t write_pass(int chunk_count, int D, const int* raw, const int* counts, const long long* offsets,
-                       unsigned char* out, int* err, cudaStream_t st)
+                       unsigned char* out, int* err, const int* inv, cudaStream_t st)
 {
     const size_t smem = (size_t)WARPS * (IDS + RUNS) * sizeof(uint32_t);
     cudaError_t e = cudaFuncSetAttribute(k_barle_write<IDS, RUNS, WARPS, LARGE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_barle_write<IDS, RUNS, WARPS, LARGE><<<(chunk_count + WARPS - 1) / WARPS, WARPS * 32, smem, st>>>(
-        chunk_count, D, raw, counts, offsets, out, err);
+        chunk_count, D, raw, counts, offsets, out, err, inv);
     return cudaGetLastError();
+}
+
+cudaError_t launch_barle_size(int chunk_count, int D, int* raw, const int* counts, int* sizes, int* err,
+                              const int* perm, cudaStream_t st)
+{
+    if (chunk_count <= 0) return cudaSuccess;
+    cudaError_t e = size_pass<kSmallIds, kSmallIds, kSmallWarps, false>(chunk_count, D, raw, counts, sizes, err,
+                                                                        perm, st);
+    if (e != cudaSuccess) return e;
+    return size_pass<kIdsCap, kRunsCap, kEncWarps, true>(chunk_count, D, raw, counts, sizes, err, perm, st);
+}
+
+cudaError_t launch_barle_write(int chunk_count, int D, const int* raw, const int* counts,
+                               const long long* offsets, unsigned char* out, int* err, const int* inv,
+                               cudaStream_t st)
+{
+    if (chunk_count <= 0) return cudaSuccess;
+    cudaError_t e = write_pass<kSmallIds, kSmallIds, kSmallWarps, false>(chunk_count, D, raw, counts, offsets,
+                                                                         out, err, inv, st);
+    if (e != cudaSuccess) return e;
+    return write_pass<kIdsCap, kRunsCap, kEncWarps, true>(chunk_count, D, raw, counts, offsets, out, err, inv, st);
 }
 
 cudaError_t launch_barle_size(int chunk_count, int D, int* raw, const int* counts,
                               int* sizes, int* err, cudaStream_t st)
 {
-    if (chunk_count <= 0) return cudaSuccess;
-    cudaError_t e = size_pass<kSmallIds, kSmallIds, kSmallWarps, false>(chunk_count, D, raw, counts, sizes, err, st);
-    if (e != cudaSuccess) return e;
-    return size_pass<kIdsCap, kRunsCap, kEncWarps, true>(chunk_count, D, raw, counts, sizes, err, st);
+    return launch_barle_size(chunk_count, D, raw, counts, sizes, err, nullptr, st);
 }
 
 cudaError_t launch_barle_write(int chunk_count, int D, const int* raw, const int* counts,
                                const long long* offsets, unsigned char* out, int* err,
                                cudaStream_t st)
 {
-    if (chunk_count <= 0) return cudaSuccess;
-    cudaError_t e = write_pass<kSmallIds, kSmallIds, kSmallWarps, false>(chunk_count, D, raw, counts, offsets,
-                                                                         out, err, st);
-    if (e != cudaSuccess) return e;
-    return write_pass<kIdsCap, kRunsCap, kEncWarps, true>(chunk_count, D, raw, counts, offsets, out, err, st);
+    return launch_barle_write(chunk_count, D, raw, counts, offsets, out, err, nullptr, st);
 }
 
 }  // namespace sgb

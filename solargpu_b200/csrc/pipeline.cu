@@ -82,7 +82,7 @@ struct solar_gpu_context {
         counts, csr_off, csr_ids, barle_off, barle_sizes, barle_bytes, scan_tmp, slab, hourly,
         acc_f64, acc_f32, acc_comp, sums, out_f64, err, in_grid, in_pp, in_wz, in_slopes,
         in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
-        grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first;
+        grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
@@ -324,17 +324,28 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         RK(ensure(c->barle_bytes, (size_t)N * 160));
     }
     const DevScene ds = dev_scene(s);
+    // One chunk: rows follow the visiting order (Morton-adjacent voxels share
+    // a warp, so their rays have similar lengths).  Several chunks: index order.
+    const int* perm = nullptr;
+    const int* inv = nullptr;
+    if (chunk >= N) {
+        RK(ensure(c->order_inv, sizeof(int) * (size_t)N));
+        CK(launch_invert(as<int>(c->order), N, as<int>(c->order_inv), st));
+        perm = as<int>(c->order);
+        inv = as<int>(c->order_inv);
+        c->launches += 1;
+    }
     long long csr_total = 0, barle_total = 0;
     for (long long v0 = 0; v0 < N; v0 += chunk) {
         const int n = (int)((N - v0) < chunk ? (N - v0) : chunk);
         {
             KScope k(c, SOLAR_GPU_KT_TRACE);
             CK(launch_trace(ds, as<DirEntry>(c->dirs), D, c->words32, (int)v0, n, as<int>(c->raw),
-                            as<uint32_t>(c->shadow), st));
+                            as<uint32_t>(c->shadow), perm, st));
         }
         {
             KScope k(c, SOLAR_GPU_KT_DEDUPE);
-            CK(launch_dedupe(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->err), st));
+            CK(launch_dedupe(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->err), perm, st));
         }
         c->launches += 2;
         const double frac_left = (double)N / (double)(v0 + n);
@@ -350,7 +361,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
             RK(ensure_keep(c->csr_ids, sizeof(int) * (size_t)(est > total ? est : total), sizeof(int) * (size_t)csr_total, st));
             {
                 KScope k(c, SOLAR_GPU_KT_CSR);
-                CK(launch_gather_csr(n, D, as<int>(c->raw), off, as<int>(c->csr_ids), st));
+                CK(launch_gather_csr(n, D, as<int>(c->raw), off, as<int>(c->csr_ids), inv, st));
             }
             csr_total = total;
             c->launches += 4;
@@ -360,7 +371,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
             {
                 KScope k(c, SOLAR_GPU_KT_BARLE);
                 CK(launch_barle_size(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->barle_sizes) + v0,
-                                     as<int>(c->err), st));
+                                     as<int>(c->err), perm, st));
                 CK(launch_scan_counts(as<int>(c->barle_sizes) + v0, n, barle_total, off, as<long long>(c->scan_tmp), nullptr, st));
             }
             long long total = 0;
@@ -370,7 +381,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
             {
                 KScope k(c, SOLAR_GPU_KT_BARLE);
                 CK(launch_barle_write(n, D, as<int>(c->raw), as<int>(c->counts) + v0, off,
-                                      as<unsigned char>(c->barle_bytes), as<int>(c->err), st));
+                                      as<unsigned char>(c->barle_bytes), as<int>(c->err), inv, st));
             }
             barle_total = total;
             c->launches += 5;
@@ -569,6 +580,7 @@ int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const sola
     c->launches = 0;
     c->timed = false;
     c->ktime = o->time_kernels != 0;
+    c->group_entries = 0;
     c->kt_used = 0;
     c->kt_ids.clear();
     c->kt_stream = st;
@@ -671,7 +683,7 @@ void solar_gpu_destroy(solar_gpu_context* c)
                       &c->in_pp, &c->in_wz, &c->in_slopes, &c->in_aspects, &c->out_f32, &c->order,
                       &c->order_cnt, &c->order_cur, &c->order_tmp, &c->grp_cnt, &c->grp_off,
                       &c->grp_tmp, &c->grp_cell, &c->grp_w, &c->w_cnt, &c->w_off, &c->w_tmp,
-                      &c->w_cell, &c->w_val, &c->order_first};
+                      &c->w_cell, &c->w_val, &c->order_first, &c->order_inv};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (cudaEvent_t e : c->kt_pool) cudaEventDestroy(e);
@@ -774,6 +786,8 @@ int solar_gpu_last_timings(solar_gpu_context* c, double* ms, int n)
 }
 
 long long solar_gpu_last_launch_count(solar_gpu_context* c) { return c ? c->launches : -1; }
+
+long long solar_gpu_last_reflection_entries(solar_gpu_context* c) { return c ? c->group_entries : -1; }
 
 int solar_gpu_kernel_times(solar_gpu_context* c, double* ms, long long* launches, int n)
 {

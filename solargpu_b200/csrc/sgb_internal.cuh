@@ -65,19 +65,29 @@ void set_last_error(const char* msg);
 // ------------------------------------------------------------------ launchers
 
 // tracer (trace.cu)
+// Stage 1 kernels address rows of the raw hit buffer.  Row lv holds voxel
+// perm[lv] when a permutation is given (counts, sizes indexed by voxel),
+// else voxel voxel_offset + lv; kernels that iterate voxels take the inverse.
 cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
                          int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
-                         cudaStream_t st);
-cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, cudaStream_t st);
+                         const int* perm, cudaStream_t st);
+cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, const int* perm,
+                          cudaStream_t st);
+cudaError_t launch_invert(const int* perm, int n, int* inv, cudaStream_t st);
 cudaError_t launch_scan_counts(const int* counts, int n, long long base, long long* offsets,
                                long long* block_sums, int* block_tmp, cudaStream_t st);
 size_t scan_scratch_elems(int n);
 cudaError_t launch_gather_csr(int chunk_count, int D, const int* raw, const long long* offsets,
-                              int* csr_ids, cudaStream_t st);
+                              int* csr_ids, const int* inv, cudaStream_t st);
 
 // ba-RLE encoder (barle.cu)
 cudaError_t launch_barle_size(int chunk_count, int D, int* raw, const int* counts,
                               int* sizes, int* err, cudaStream_t st);
+cudaError_t launch_barle_size(int chunk_count, int D, int* raw, const int* counts, int* sizes, int* err,
+                              const int* perm, cudaStream_t st);
+cudaError_t launch_barle_write(int chunk_count, int D, const int* raw, const int* counts,
+                               const long long* offsets, unsigned char* out, int* err, const int* inv,
+                               cudaStream_t st);
 cudaError_t launch_barle_write(int chunk_count, int D, const int* raw, const int* counts,
                                const long long* offsets, unsigned char* out, int* err,
                                cudaStream_t st);

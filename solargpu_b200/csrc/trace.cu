@@ -60,12 +60,15 @@ __device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, 
 
 __global__ void __launch_bounds__(kTraceBlock)
 k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
-        int voxel_offset, int chunk_count, int* __restrict__ raw, uint32_t* __restrict__ shadow)
+        int voxel_offset, int chunk_count, int* __restrict__ raw, uint32_t* __restrict__ shadow,
+        const int* __restrict__ perm)
 {
     __shared__ int stage[kRawGroup][kTraceBlock];
     const int lv = blockIdx.x * kTraceBlock + threadIdx.x;
     const bool active = lv < chunk_count;
-    const int v = voxel_offset + (active ? lv : 0);
+    // Row lv traces voxel perm[lv] (visiting order: Morton-adjacent lanes walk
+    // similar rays) or voxel_offset + lv.
+    const int v = perm ? __ldg(perm + (active ? lv : 0)) : voxel_offset + (active ? lv : 0);
     const int top = __ldg(s.pix_parent + v);
     const int gx = top % s.W;
     const int gy = top / s.W;
@@ -110,7 +113,8 @@ __device__ __forceinline__ uint32_t hash_slot(uint32_t x)
 // One warp per voxel: keeps the first occurrence of each hit id in direction
 // order and compacts the row in place; counts[lv] = list length.
 __global__ void __launch_bounds__(kDedupeWarps * 32)
-k_dedupe(int chunk_count, int D, int* __restrict__ raw, int* __restrict__ counts, int* __restrict__ err)
+k_dedupe(int chunk_count, int D, int* __restrict__ raw, int* __restrict__ counts, int* __restrict__ err,
+         const int* __restrict__ perm)
 {
     extern __shared__ uint32_t tab_all[];
     const int warp = threadIdx.x >> 5;
@@ -155,7 +159,7 @@ k_dedupe(int chunk_count, int D, int* __restrict__ raw, int* __restrict__ counts
             n += __popc(bal);
         }
     }
-    if (lane == 0) counts[lv] = n;
+    if (lane == 0) counts[perm ? perm[lv] : lv] = n;
 }
 
 // ---- exclusive scan of int counts into int64 offsets (3 phases) ----------
@@ -240,14 +244,14 @@ __global__ void k_scan_add(long long* __restrict__ offsets, int n, const long lo
 
 __global__ void __launch_bounds__(256)
 k_gather_csr(int chunk_count, int D, const int* __restrict__ raw, const long long* __restrict__ offsets,
-             int* __restrict__ csr_ids)
+             int* __restrict__ csr_ids, const int* __restrict__ inv)
 {
     const int lv = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (lv >= chunk_count) return;
     const long long o = offsets[lv];
     const int k = (int)(offsets[lv + 1] - o);
-    const int* row = raw + (size_t)lv * D;
+    const int* row = raw + (size_t)(inv ? inv[lv] : lv) * D;
     for (int i = lane; i < k; i += 32) csr_ids[o + i] = row[i];
 }
 
@@ -255,22 +259,23 @@ k_gather_csr(int chunk_count, int D, const int* __restrict__ raw, const long lon
 
 cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
                          int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
-                         cudaStream_t st)
+                         const int* perm, cudaStream_t st)
 {
     if (chunk_count <= 0) return cudaSuccess;
     const int grid = (chunk_count + kTraceBlock - 1) / kTraceBlock;
-    k_trace<<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow);
+    k_trace<<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow, perm);
     return cudaGetLastError();
 }
 
-cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, cudaStream_t st)
+cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, const int* perm,
+                          cudaStream_t st)
 {
     if (chunk_count <= 0) return cudaSuccess;
     const size_t smem = (size_t)kDedupeWarps * kHashSlots * sizeof(uint32_t);
     cudaError_t e = cudaFuncSetAttribute(k_dedupe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (chunk_count + kDedupeWarps - 1) / kDedupeWarps;
-    k_dedupe<<<grid, kDedupeWarps * 32, smem, st>>>(chunk_count, D, raw, counts, err);
+    k_dedupe<<<grid, kDedupeWarps * 32, smem, st>>>(chunk_count, D, raw, counts, err, perm);
     return cudaGetLastError();
 }
 
@@ -290,11 +295,26 @@ cudaError_t launch_scan_counts(const int* counts, int n, long long base, long lo
 }
 
 cudaError_t launch_gather_csr(int chunk_count, int D, const int* raw, const long long* offsets,
-                              int* csr_ids, cudaStream_t st)
+                              int* csr_ids, const int* inv, cudaStream_t st)
 {
     if (chunk_count <= 0) return cudaSuccess;
     const long long threads = (long long)chunk_count * 32;
-    k_gather_csr<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(chunk_count, D, raw, offsets, csr_ids);
+    k_gather_csr<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(chunk_count, D, raw, offsets, csr_ids, inv);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void k_invert(const int* __restrict__ perm, int n, int* __restrict__ inv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) inv[perm[i]] = i;
+}
+}  // namespace
+
+cudaError_t launch_invert(const int* perm, int n, int* inv, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    k_invert<<<(n + 255) / 256, 256, 0, st>>>(perm, n, inv);
     return cudaGetLastError();
 }
 
