@@ -1,0 +1,59 @@
+"""Command-line runner: the annual irradiance path on a named synthetic workload.
+
+    python -m solargpu_b200.run --workload dsm1024 [--format 1] [--hour-block 256]
+                                [--group-size 1] [--accumulation 1] [--runs 2] [--out file.npy]
+
+Plays the role of the reference CLI (src/main.cpp) for generated scenes:
+builds the seeded DSM, voxelizes it, computes the sun series and TMY, runs
+the CUDA pipeline `--runs` times on device-resident inputs and prints the
+stage and kernel-group times of the last run.  Also the profiling driver
+(run it under ncu with -k/-s/-c filters).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+
+import numpy as np
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--workload", default="dsm1024")
+    ap.add_argument("--format", type=int, default=1, help="0 = CSR, 1 = ba-RLE")
+    ap.add_argument("--hour-block", type=int, default=256)
+    ap.add_argument("--group-size", type=int, default=1)
+    ap.add_argument("--accumulation", type=int, default=1)
+    ap.add_argument("--chunk-voxels", type=int, default=0)
+    ap.add_argument("--runs", type=int, default=2)
+    ap.add_argument("--out", default=None, help="write the annual irradiance (float32 .npy)")
+    a = ap.parse_args(argv)
+
+    import torch
+    from solargpu_b200 import api, inputs
+
+    s = inputs.make_scene(a.workload)
+    dev = torch.device("cuda:0")
+    d = {"grid": torch.from_numpy(s.grid).to(dev), "pixel_parent": torch.from_numpy(s.pixel_parent).to(dev),
+         "wall_z": torch.from_numpy(s.wall_z if s.wall_z.size else np.zeros(1, np.float32)).to(dev),
+         "slopes": torch.from_numpy(s.slopes).to(dev), "aspects": torch.from_numpy(s.aspects).to(dev)}
+    out = torch.zeros(s.num_total, dtype=torch.float32, device=dev)
+    with api.Context(0) as ctx:
+        for _ in range(max(1, a.runs)):
+            ctx.run_device(s, d, out, neighbor_format=a.format, hour_block=a.hour_block,
+                           group_size=a.group_size, accumulation=a.accumulation,
+                           chunk_voxels=a.chunk_voxels, use_graph=0, time_kernels=1)
+            torch.cuda.synchronize()
+        t = ctx.timings()
+        kt = {k: round(v[0], 3) for k, v in ctx.kernel_times().items() if v[1]}
+    print(json.dumps({"workload": a.workload, "voxels": s.num_total, "top_voxels": s.num_top,
+                      "stage_ms": {"setup": round(t[0], 3), "stage1": round(t[1], 3), "stage23": round(t[2], 3),
+                                   "total": round(t[3], 3)}, "kernel_group_ms": kt}))
+    if a.out:
+        np.save(a.out, out.cpu().numpy())
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
