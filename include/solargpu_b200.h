@@ -60,7 +60,9 @@ typedef struct solar_gpu_options {
                                 and weights computed in every block (B 32..256); 1 = weights computed
                                 once per run (B 64..512); 2, 4, 8 = that many voxels share one warp,
                                 their weighted lists merged once per run into union entries
-                                (B 64..512, 32..256, 32..128) */
+                                (B 64..512, 32..256, 32..128); 64 = groups of up to 64 voxels
+                                whose union rows are staged through shared memory, one CTA
+                                per group (B 64..256) */
 } solar_gpu_options;
 
 void solar_gpu_default_options(solar_gpu_options* opt);
@@ -97,6 +99,10 @@ typedef struct solar_gpu_context solar_gpu_context;
 
 int solar_gpu_create(int device, solar_gpu_context** out);
 void solar_gpu_destroy(solar_gpu_context* ctx);
+/* Frees the context's device buffers (they are grow-only and otherwise kept
+   for the next call); the context stays usable.  Results of the last trace
+   are no longer available afterwards. */
+int solar_gpu_release(solar_gpu_context* ctx);
 
 /* Scene description.  For solar_gpu_run_host the array pointers are host
    pointers; for solar_gpu_run_device and solar_gpu_trace the per-cell and

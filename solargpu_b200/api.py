@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
         L.solar_gpu_create.argtypes = [i, C.POINTER(vp)]
         L.solar_gpu_destroy.argtypes = [vp]
         L.solar_gpu_destroy.restype = None
+        L.solar_gpu_release.argtypes = [vp]
         L.solar_gpu_default_options.argtypes = [C.POINTER(Options)]
         L.solar_gpu_default_options.restype = None
         L.solar_gpu_run_host.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), vp]
@@ -201,6 +202,10 @@ class Context:
         if getattr(self, "h", None) and self.h.value:
             lib().solar_gpu_destroy(self.h)
             self.h = C.c_void_p()
+
+    def release(self):
+        """Frees the device buffers kept between calls (solar_gpu_release)."""
+        _check(lib().solar_gpu_release(self.h))
 
     def __enter__(self):
         return self

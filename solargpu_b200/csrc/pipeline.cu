@@ -82,7 +82,8 @@ struct solar_gpu_context {
         counts, csr_off, csr_ids, barle_off, barle_sizes, barle_bytes, scan_tmp, slab, hourly,
         acc_f64, acc_f32, acc_comp, sums, out_f64, err, in_grid, in_pp, in_wz, in_slopes,
         in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
-        grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv;
+        grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
+        tile_start, tile_union, tile_slot;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
@@ -200,7 +201,8 @@ int check_options(const solar_gpu_options* o, bool trace_only)
     case 0: case 4: ok = Bq >= 32 && Bq <= 256; break;
     case 8: ok = Bq >= 32 && Bq <= 128; break;
     case 1: case 2: ok = Bq >= 64 && Bq <= 512; break;
-    default: return fail(SOLAR_GPU_ERR_ARG, "group_size %d (0, 1, 2, 4 or 8)", V);
+    case 64: ok = Bq >= 64 && Bq <= 256; break;
+    default: return fail(SOLAR_GPU_ERR_ARG, "group_size %d (0, 1, 2, 4, 8 or 64)", V);
     }
     if (Bq > 1 && !ok)
         return fail(SOLAR_GPU_ERR_ARG, "hour_block %d is not built for group_size %d", Bq, V);
@@ -464,6 +466,8 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         RK(ensure(c->slab, sizeof(float) * (size_t)T * B));
         float* slab = as<float>(c->slab);
         GroupLists gl{o->group_size, nullptr, nullptr, nullptr};
+        TileLists tl{};
+        const bool tiled = o->group_size >= 64;
         if (o->group_size > 0) {
             // Once per run: the nonzero weights of every list in visiting order,
             // then (V > 1) the merged union entries of each group of V voxels.
@@ -493,6 +497,38 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 gl.offsets = as<long long>(c->w_off);
                 gl.cells = as<int>(c->w_cell);
                 gl.weights = as<float>(c->w_val);
+            } else if (tiled) {
+                // Groups of up to V visiting positions; the weighted lists of
+                // each group are rewritten in place into union cells + slots.
+                RK(ensure(c->tile_flag, sizeof(int) * (size_t)N));
+                RK(ensure(c->tile_pos, sizeof(long long) * ((size_t)N + 1)));
+                RK(ensure(c->tile_start, sizeof(int) * ((size_t)N + 1)));
+                RK(ensure(c->tile_slot, sizeof(unsigned short) * (size_t)(Ew + 1)));
+                {
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(launch_tile_groups(N, V, as<long long>(c->w_off), as<int>(c->tile_flag),
+                                          as<long long>(c->tile_pos), as<long long>(c->w_tmp),
+                                          as<int>(c->tile_start), st));
+                }
+                long long NG = 0;
+                RK(read_ll(c, as<long long>(c->tile_pos) + N, &NG, st));
+                RK(ensure(c->tile_union, sizeof(int) * (size_t)(NG + 1)));
+                {
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(launch_tile_build((int)NG, as<int>(c->tile_start), as<long long>(c->w_off),
+                                         as<int>(c->w_cell), as<float>(c->w_val),
+                                         as<unsigned short>(c->tile_slot), as<int>(c->tile_union), err, st));
+                }
+                c->launches += 5;
+                c->group_entries = Ew;
+                tl.G = V;
+                tl.NG = (int)NG;
+                tl.start = as<int>(c->tile_start);
+                tl.unions = as<int>(c->tile_union);
+                tl.woff = as<long long>(c->w_off);
+                tl.cells = as<int>(c->w_cell);
+                tl.slots = as<unsigned short>(c->tile_slot);
+                tl.weights = as<float>(c->w_val);
             } else {
                 const int G = group_count(N, V);
                 RK(ensure(c->grp_cnt, sizeof(int) * (size_t)G));
@@ -534,7 +570,10 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
             }
             if (le == cudaSuccess) {
                 KScope k(c, SOLAR_GPU_KT_REFLECT);
-                if (o->group_size > 0)
+                if (tiled)
+                    le = launch_reflect_tile(g, sh, c->words32, tab, j0, B, slab, tl, as<int>(c->order), acc, err,
+                                             st);
+                else if (o->group_size > 0)
                     le = launch_reflect_group(g, N, sh, c->words32, tab, j0, B, slab, gl, as<int>(c->order), acc, st);
                 else
                     le = launch_reflect_block(g, N, T, sh, c->words32, tab, j0, B, slab, nl, acc,
@@ -566,7 +605,7 @@ int check_device_flags(solar_gpu_context* c, cudaStream_t st)
     CK(cudaStreamSynchronize(st));
     int f = 0;
     std::memcpy(&f, c->h_scalars, sizeof(int));
-    if (f) return fail(SOLAR_GPU_ERR_DEVICE_CHECK, "device check flags 0x%x (1 = ba-RLE stream, 2 = hash, 4 = capacity)", f);
+    if (f) return fail(SOLAR_GPU_ERR_DEVICE_CHECK, "device check flags 0x%x (1 = ba-RLE stream, 2 = hash, 4 = capacity, 8 = wait timeout)", f);
     return SOLAR_GPU_OK;
 }
 
@@ -671,19 +710,48 @@ int solar_gpu_create(int device, solar_gpu_context** out)
     return SOLAR_GPU_OK;
 }
 
-void solar_gpu_destroy(solar_gpu_context* c)
+static constexpr int kNumBufs = 53;
+
+static void all_bufs(solar_gpu_context* c, DevBuf** out)
 {
-    if (!c) return;
-    cudaSetDevice(c->device);
-    if (c->own) cudaStreamSynchronize(c->own);
-    DevBuf* bufs[] = {&c->dirs, &c->nudged, &c->dni, &c->dhi, &c->sun_dense, &c->hour_index, &c->table,
+    DevBuf* bufs[kNumBufs] = {&c->dirs, &c->nudged, &c->dni, &c->dhi, &c->sun_dense, &c->hour_index, &c->table,
                       &c->geo_n, &c->geo_p, &c->shadow, &c->raw, &c->counts, &c->csr_off, &c->csr_ids,
                       &c->barle_off, &c->barle_sizes, &c->barle_bytes, &c->scan_tmp, &c->slab, &c->hourly,
                       &c->acc_f64, &c->acc_f32, &c->acc_comp, &c->sums, &c->out_f64, &c->err, &c->in_grid,
                       &c->in_pp, &c->in_wz, &c->in_slopes, &c->in_aspects, &c->out_f32, &c->order,
                       &c->order_cnt, &c->order_cur, &c->order_tmp, &c->grp_cnt, &c->grp_off,
                       &c->grp_tmp, &c->grp_cell, &c->grp_w, &c->w_cnt, &c->w_off, &c->w_tmp,
-                      &c->w_cell, &c->w_val, &c->order_first, &c->order_inv};
+                      &c->w_cell, &c->w_val, &c->order_first, &c->order_inv,
+                                &c->tile_flag, &c->tile_pos, &c->tile_start, &c->tile_union, &c->tile_slot};
+    for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
+}
+
+int solar_gpu_release(solar_gpu_context* c)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    DevBuf* bufs[kNumBufs];
+    all_bufs(c, bufs);
+    for (DevBuf* b : bufs) {
+        if (b->p) cudaFree(b->p);
+        b->p = nullptr;
+        b->cap = 0;
+    }
+    c->have_csr = c->have_barle = false;
+    c->N = 0;
+    c->timed = false;
+    c->kt_used = 0;
+    return SOLAR_GPU_OK;
+}
+
+void solar_gpu_destroy(solar_gpu_context* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->own) cudaStreamSynchronize(c->own);
+    DevBuf* bufs[kNumBufs];
+    all_bufs(c, bufs);
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (cudaEvent_t e : c->kt_pool) cudaEventDestroy(e);

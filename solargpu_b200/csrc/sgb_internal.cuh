@@ -18,6 +18,7 @@ enum DeviceError : int {
     kErrBarleStream = 1,   // a ba-RLE stream ran past its byte range or had a bad width code
     kErrHashFull = 2,      // a dedupe hash probe exceeded its bound
     kErrListCapacity = 4,  // a neighbor list exceeded the buffer capacity
+    kErrWaitTimeout = 8,   // a bounded wait on a shared-memory barrier expired
 };
 
 // One traced direction; host-computed exactly as the reference computes Cdir
@@ -155,5 +156,26 @@ cudaError_t launch_reflect_group(const DevGeom& g, int N, const uint32_t* shadow
                                  const HourEntry* table, int j0, int B, const float* slab,
                                  const GroupLists& gl, const int* order, const Accum& acc, cudaStream_t st);
 cudaError_t launch_finalize_f64(const double* in, int N, float* out, cudaStream_t st);
+
+// tiled reflection (tile.cu)
+struct TileLists {
+    int G;                         // voxels per group at most (64)
+    int NG;                        // groups
+    const int* start;              // [NG + 1] first visiting position of each group
+    const int* unions;             // [NG] union rows of each group
+    const long long* woff;         // [N + 1] entry offsets per visiting position
+    const int* cells;              // union cells of group q at woff[start[q]] (descending)
+    const unsigned short* slots;   // [E] union index of each entry, ascending per voxel
+    const float* weights;          // [E] weight of each entry
+};
+// Group boundaries: flag/pos scratch [N] / [N + 1]; start [N + 1].
+cudaError_t launch_tile_groups(int N, int G, const long long* woff, int* flag, long long* pos,
+                               long long* scan_tmp, int* start, cudaStream_t st);
+// Rewrites the weighted lists of each group in place into union + slots.
+cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, float* wts,
+                              unsigned short* slots, int* unions, int* err, cudaStream_t st);
+cudaError_t launch_reflect_tile(const DevGeom& g, const uint32_t* shadow, int words32, const HourEntry* table,
+                                int j0, int B, const float* slab, const TileLists& tl, const int* order,
+                                const Accum& acc, int* err, cudaStream_t st);
 
 }  // namespace sgb

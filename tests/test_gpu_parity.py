@@ -71,12 +71,14 @@ def test_trace_matches_reference_kernel(ctx, scene64):
 
 
 # (format, hour block, accumulation, group size): the plain per-hour path,
-# the per-voxel block kernel (group 0) and the grouped kernel (4, 8).
+# the per-voxel block kernel (group 0), the grouped kernel (1, 2, 4, 8) and
+# the shared-memory tile kernel (64).
 CASES = ([(fmt, 1, acc, 0) for fmt in (0, 1) for acc in (0, 1, 2)]
          + [(fmt, B, acc, 0) for fmt in (0, 1) for B in (32, 64, 128, 256) for acc in (0, 1, 2)]
          + [(fmt, B, acc, V) for fmt in (0, 1) for V in (4, 8) for B in (32, 64, 128, 256) for acc in (0, 1, 2)
             if not (V == 8 and B == 256)]
-         + [(fmt, B, acc, V) for fmt in (0, 1) for V in (1, 2) for B in (64, 128, 256, 512) for acc in (0, 1)])
+         + [(fmt, B, acc, V) for fmt in (0, 1) for V in (1, 2) for B in (64, 128, 256, 512) for acc in (0, 1)]
+         + [(fmt, B, acc, 64) for fmt in (0, 1) for B in (64, 128, 256) for acc in (0, 1, 2)])
 
 
 @pytest.mark.parametrize("fmt,B,acc,V", CASES)
@@ -103,7 +105,7 @@ def test_annual_form_vs_fp64(ctx, scene160, fmt):
     assert e.max() <= REL_TOL, (e.max(), e.mean())
 
 
-@pytest.mark.parametrize("fmt,V", [(0, 0), (1, 0), (0, 8), (1, 8), (1, 4), (0, 1), (1, 2)])
+@pytest.mark.parametrize("fmt,V", [(0, 0), (1, 0), (0, 8), (1, 8), (1, 4), (0, 1), (1, 2), (0, 64), (1, 64)])
 def test_hour_block_vs_fp64_dsm160(ctx, scene160, fmt, V):
     import torch
     s = scene160
@@ -160,6 +162,21 @@ def test_grouped_results_are_reproducible(ctx, scene160):
         ctx.run_device(scene160, dev, out, neighbor_format=1, hour_block=128, group_size=8)
         outs.append(out.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("B", [128, 256])
+def test_tiles_equal_per_voxel_lists_on_barle(ctx, scene160, B):
+    """The tile kernel applies each voxel's entries in the ba-RLE list order
+    with the same FMA chain, so it reproduces group size 1 bit for bit."""
+    import torch
+    dev = device_arrays(scene160)
+    outs = []
+    for V in (1, 64, 64):
+        out = torch.zeros(scene160.num_total, dtype=torch.float32, device="cuda:0")
+        ctx.run_device(scene160, dev, out, neighbor_format=1, hour_block=B, accumulation=1, group_size=V)
+        outs.append(out.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[1], outs[2])
 
 
 def test_invalid_hour_block_for_group_is_rejected(ctx, scene64):
