@@ -158,22 +158,28 @@ def workload_desc(scene, name: str) -> str:
             f"lat {c.lat} lon {c.lon} tz +{c.tz}, synthetic TMY")
 
 
-def roofline_bytes(scene, ctx_sizes, fmt, B, acc, V, entries) -> float:
+def roofline_bytes(scene, ctx_sizes, fmt, B, acc, V, entries, staged_rows=0) -> float:
     """Algorithmic HBM bytes of one hour-block reflection launch, gathered
-    slab rows counted once (as cache hits): the streamed lists (V = 0: CSR ids
-    or ba-RLE bytes + offsets; V >= 1: entries of one cell id + V weights +
-    group offsets), per voxel the visiting-order index, geometry, shadow words
-    and accumulator read/write, plus one read of the block's top-cell slab."""
+    slab rows counted once (as cache hits): the streamed lists, per voxel the
+    visiting-order index and accumulator read/write, and one read of the
+    block's slab.
+      V = 0: CSR ids or ba-RLE bytes + offsets; geometry and shadow words per
+             voxel; slab rows of the top cells.
+      V = 1, 2, 4, 8: entries of one cell id + V weights, group offsets; the
+             slab has a row for every voxel (its own term).
+      V = 64 (tiles): entries of a 2-byte slot + weight, the groups' union
+             cell ids, offsets; slab rows of every voxel."""
     csr_entries, barle_bytes, words32 = ctx_sizes
     N, T = scene.num_total, scene.num_top
     acc_b = 16 if acc in (0, 1) else 8
     if V == 0:
         lists = (barle_bytes if fmt == 1 else 4 * csr_entries) + 8 * (N + 1)
-        per_voxel = 4 + 32 + 4 * words32 + acc_b
+        return float(lists + N * (4 + 32 + 4 * words32 + acc_b) + T * B * 4)
+    if V >= 64:
+        lists = entries * 6 + staged_rows * 4 + 8 * (N + 1)
     else:
         lists = entries * (4 + 4 * V) + 8 * (N // V + 2)
-        per_voxel = 4 + 16 + 4 * words32 + acc_b
-    return float(lists + N * per_voxel + T * B * 4)
+    return float(lists + N * (4 + acc_b) + N * B * 4)
 
 
 # ---------------------------------------------------------------- our arm
@@ -255,13 +261,15 @@ def run_ours(args, world, rank, local, pg):
     B = args.hour_block
     V = args.group_size
     entries = ctx.reflection_entries()
-    alg = roofline_bytes(scene, (ne.value, nb.value, w.value), args.format, B, args.accumulation, V, entries)
+    staged = ctx.staged_rows()
+    alg = roofline_bytes(scene, (ne.value, nb.value, w.value), args.format, B, args.accumulation, V, entries, staged)
     per_launch_ms = refl_ms / max(1, refl_n)
     achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
-    # slab values moved through L1 per launch (one row of B floats per entry)
+    # slab values delivered to the FMA units per launch (one row of B floats
+    # per entry: through L1, or from shared memory for the tile kernel)
     gathered = float(entries if V >= 1 else ne.value) * B * 4
     traffic = None
-    kname = "reflect_group" if V >= 1 else "reflect_block"
+    kname = "reflect_tile" if V >= 64 else "reflect_group" if V >= 1 else "reflect_block"
     prof = os.path.join(ROOT, "profiles", f"{kname}_{args.workload}_{FMT_NAMES[args.format].replace('-', '').lower()}_b{B}_v{V}.md")
     if os.path.exists(prof):
         for ln in open(prof):
@@ -270,8 +278,13 @@ def run_ours(args, world, rank, local, pg):
                     traffic = float(ln.split(":", 1)[1].split()[0])
                 except ValueError:
                     pass
-    kdesc = (f"k_reflect_group<{B // 32},{V}> (hour-block sparse x dense product over weighted lists + accumulation)"
-             if V >= 1 else f"k_reflect_block<{B // 32},{args.format}> (hour-block sparse x dense product + accumulation)")
+    if V >= 64:
+        kdesc = (f"k_reflect_tile<{B // 32},{V // 16}> (hour-block sparse x dense product, union rows of {V}-voxel "
+                 f"groups staged in shared memory by cp.async.bulk + accumulation)")
+    elif V >= 1:
+        kdesc = f"k_reflect_group<{B // 32},{V}> (hour-block sparse x dense product over weighted lists + accumulation)"
+    else:
+        kdesc = f"k_reflect_block<{B // 32},{args.format}> (hour-block sparse x dense product + accumulation)"
     roof = {"bound": "hbm", "kernel": kdesc,
             "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 5), "peak_source": peak_src,
@@ -279,7 +292,9 @@ def run_ours(args, world, rank, local, pg):
             "share_of_step": round(refl_ms / max(1e-9, sum(v[0] for v in ktimes.values())), 4),
             "dominant_group": dom[0],
             "gathered_slab_bytes_per_launch": gathered,
-            "l1_gather_gbs": round(gathered / (per_launch_ms / 1e3) / 1e9, 1) if per_launch_ms > 0 else None}
+            "gather_gbs": round(gathered / (per_launch_ms / 1e3) / 1e9, 1) if per_launch_ms > 0 else None}
+    if V >= 64:
+        roof["staged_slab_bytes_per_launch"] = float(staged) * B * 4
 
     # ---- end to end through the host API (pinned host buffers in and out)
     e2e = None
@@ -324,6 +339,7 @@ def run_ours(args, world, rank, local, pg):
         torch.cuda.synchronize(dev)
     if rank == 0:
         # the other neighbor-list format on the same workload (both paths run here)
+        ctx.release()
         ofmt = 1 - args.format
         oopts = dict(opts, neighbor_format=ofmt, time_kernels=0)
         ctx.run_device(scene, d, out, stream=stream.cuda_stream, **oopts)

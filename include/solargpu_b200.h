@@ -181,6 +181,11 @@ int solar_gpu_kernel_times(solar_gpu_context* ctx, double* ms, long long* launch
    (weighted or merged union entries; 0 for group_size 0). */
 long long solar_gpu_last_reflection_entries(solar_gpu_context* ctx);
 
+/* Slab rows the shared-memory tile kernel (group_size 64) staged per hour
+   block in the last run: the sum over groups of their union sizes; 0 for
+   other kernels. */
+long long solar_gpu_last_staged_rows(solar_gpu_context* ctx);
+
 /* Number of kernel launches the library issued in the last run. */
 long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
 

@@ -302,10 +302,9 @@ __device__ __forceinline__ void accumulate_g(const Accum& a, int v, float x)
 
 template <int Q, int V>
 __global__ void __launch_bounds__(kGroupWarps * 32)
-k_reflect_group(const float4* __restrict__ geo_n, int N, const uint32_t* __restrict__ shadow, int words32,
-                const HourEntry* __restrict__ table, int j0, const float* __restrict__ slab,
-                const long long* __restrict__ goff, const int* __restrict__ gcell,
-                const float* __restrict__ gw, const int* __restrict__ order, Accum acc)
+k_reflect_group(int N, const float* __restrict__ slab, const long long* __restrict__ goff,
+                const int* __restrict__ gcell, const float* __restrict__ gw, const int* __restrict__ order,
+                Accum acc)
 {
     __shared__ int s_cell[kGroupWarps][32];
     __shared__ __align__(16) float s_w[kGroupWarps][32][V];
@@ -359,14 +358,14 @@ k_reflect_group(const float4* __restrict__ geo_n, int N, const uint32_t* __restr
 #pragma unroll
         for (int s = 0; s < V; ++s) {
             if (s < gs) {
+                // the voxel's own direct + diffuse: its slab row (k_solar_slab
+                // computes rows for every voxel when the slab serves this kernel)
                 const int v = __ldg(order + q * V + s);
-                const float4 n4 = __ldg(geo_n + v);
+                float own[Q];
+                load_row<Q>(own, slab + (size_t)v * (32 * Q), lane);
                 float sum = 0.0f;
 #pragma unroll
-                for (int h = 0; h < Q; ++h) {
-                    const HourEntry e = table[j0 + lane_hour(Q, lane, h)];
-                    sum += solar_I(n4, e, shadow_bit(shadow, words32, v, e.dense)) + a[s][h];
-                }
+                for (int h = 0; h < Q; ++h) sum += own[h] + a[s][h];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
                 if (lane == 0) accumulate_g(acc, v, sum);
@@ -402,16 +401,15 @@ cudaError_t merge_pass(int N, const long long* woff, const int* wcell, const flo
 }
 
 template <int Q, int V>
-cudaError_t group_q(const DevGeom& g, int N, const uint32_t* shadow, int words32, const HourEntry* table,
-                    int j0, const float* slab, const GroupLists& gl, const int* order, const Accum& acc,
+cudaError_t group_q(int N, const float* slab, const GroupLists& gl, const int* order, const Accum& acc,
                     cudaStream_t st)
 {
     const int G = (N + V - 1) / V;
     const long long need = ((long long)G + kGroupWarps - 1) / kGroupWarps;
     const long long cap = (long long)sm_count() * 8;
     const int grid = (int)(need < cap ? need : cap);
-    k_reflect_group<Q, V><<<grid, kGroupWarps * 32, 0, st>>>(g.geo_n, N, shadow, words32, table, j0, slab,
-                                                              gl.offsets, gl.cells, gl.weights, order, acc);
+    k_reflect_group<Q, V><<<grid, kGroupWarps * 32, 0, st>>>(N, slab, gl.offsets, gl.cells, gl.weights, order,
+                                                              acc);
     return cudaGetLastError();
 }
 
@@ -452,43 +450,42 @@ cudaError_t launch_group_merge(int pass, int V, int N, const long long* woff, co
     }
 }
 
-cudaError_t launch_reflect_group(const DevGeom& g, int N, const uint32_t* shadow, int words32,
-                                 const HourEntry* table, int j0, int B, const float* slab,
-                                 const GroupLists& gl, const int* order, const Accum& acc, cudaStream_t st)
+cudaError_t launch_reflect_group(int N, int B, const float* slab, const GroupLists& gl, const int* order,
+                                 const Accum& acc, cudaStream_t st)
 {
     if (N <= 0) return cudaSuccess;
     if (gl.V == 8) {
         switch (B) {
-        case 32: return group_q<1, 8>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 64: return group_q<2, 8>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 128: return group_q<4, 8>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 32: return group_q<1, 8>(N, slab, gl, order, acc, st);
+        case 64: return group_q<2, 8>(N, slab, gl, order, acc, st);
+        case 128: return group_q<4, 8>(N, slab, gl, order, acc, st);
         default: return cudaErrorInvalidValue;
         }
     }
     if (gl.V == 4) {
         switch (B) {
-        case 32: return group_q<1, 4>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 64: return group_q<2, 4>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 128: return group_q<4, 4>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 256: return group_q<8, 4>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 32: return group_q<1, 4>(N, slab, gl, order, acc, st);
+        case 64: return group_q<2, 4>(N, slab, gl, order, acc, st);
+        case 128: return group_q<4, 4>(N, slab, gl, order, acc, st);
+        case 256: return group_q<8, 4>(N, slab, gl, order, acc, st);
         default: return cudaErrorInvalidValue;
         }
     }
     if (gl.V == 2) {
         switch (B) {
-        case 64: return group_q<2, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 128: return group_q<4, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 256: return group_q<8, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 512: return group_q<16, 2>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 64: return group_q<2, 2>(N, slab, gl, order, acc, st);
+        case 128: return group_q<4, 2>(N, slab, gl, order, acc, st);
+        case 256: return group_q<8, 2>(N, slab, gl, order, acc, st);
+        case 512: return group_q<16, 2>(N, slab, gl, order, acc, st);
         default: return cudaErrorInvalidValue;
         }
     }
     if (gl.V == 1) {
         switch (B) {
-        case 64: return group_q<2, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 128: return group_q<4, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 256: return group_q<8, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
-        case 512: return group_q<16, 1>(g, N, shadow, words32, table, j0, slab, gl, order, acc, st);
+        case 64: return group_q<2, 1>(N, slab, gl, order, acc, st);
+        case 128: return group_q<4, 1>(N, slab, gl, order, acc, st);
+        case 256: return group_q<8, 1>(N, slab, gl, order, acc, st);
+        case 512: return group_q<16, 1>(N, slab, gl, order, acc, st);
         default: return cudaErrorInvalidValue;
         }
     }

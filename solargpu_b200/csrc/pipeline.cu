@@ -83,7 +83,7 @@ struct solar_gpu_context {
         acc_f64, acc_f32, acc_comp, sums, out_f64, err, in_grid, in_pp, in_wz, in_slopes,
         in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
-        tile_start, tile_union, tile_slot;
+        tile_start, tile_union, tile_slot, tile_rows;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
@@ -92,6 +92,7 @@ struct solar_gpu_context {
     double timings[4] = {0, 0, 0, 0};
     long long launches = 0;
     long long group_entries = 0;
+    long long staged_rows = 0;   // slab rows the tile kernel stages per hour block
     bool timed = false;
     // per kernel-group event log (time_kernels)
     bool ktime = false;
@@ -391,6 +392,16 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     }
     c->csr_total = csr_total;
     c->barle_total = barle_total;
+    // A raw hit buffer above a quarter of the device (scenes of tens of
+    // millions of voxels) is released here to leave room for Stage 2/3;
+    // smaller ones are kept for the next call.
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    if (c->raw.cap > tot / 4) {
+        CK(cudaFree(c->raw.p));
+        c->raw.p = nullptr;
+        c->raw.cap = 0;
+    }
     return SOLAR_GPU_OK;
 }
 
@@ -463,7 +474,10 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         }
         c->launches += 2LL * Hd;
     } else {
-        RK(ensure(c->slab, sizeof(float) * (size_t)T * B));
+        // Rows for the top cells (neighbor values); the weighted-list kernels
+        // also read each voxel's own row, so there the slab covers all voxels.
+        const int slab_rows = o->group_size > 0 ? N : T;
+        RK(ensure(c->slab, sizeof(float) * (size_t)slab_rows * B));
         float* slab = as<float>(c->slab);
         GroupLists gl{o->group_size, nullptr, nullptr, nullptr};
         TileLists tl{};
@@ -513,12 +527,15 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 long long NG = 0;
                 RK(read_ll(c, as<long long>(c->tile_pos) + N, &NG, st));
                 RK(ensure(c->tile_union, sizeof(int) * (size_t)(NG + 1)));
+                RK(ensure(c->tile_rows, sizeof(long long)));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(launch_tile_build((int)NG, as<int>(c->tile_start), as<long long>(c->w_off),
                                          as<int>(c->w_cell), as<float>(c->w_val),
-                                         as<unsigned short>(c->tile_slot), as<int>(c->tile_union), err, st));
+                                         as<unsigned short>(c->tile_slot), as<int>(c->tile_union),
+                                         as<long long>(c->tile_rows), err, st));
                 }
+                RK(read_ll(c, as<long long>(c->tile_rows), &c->staged_rows, st));
                 c->launches += 5;
                 c->group_entries = Ew;
                 tl.G = V;
@@ -566,15 +583,14 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         for (int j0 = 0; j0 < Hd && le == cudaSuccess; j0 += B) {
             {
                 KScope k(c, SOLAR_GPU_KT_SOLAR);
-                le = launch_solar_slab(g, T, sh, c->words32, tab, j0, B, slab, st);
+                le = launch_solar_slab(g, slab_rows, sh, c->words32, tab, j0, B, slab, st);
             }
             if (le == cudaSuccess) {
                 KScope k(c, SOLAR_GPU_KT_REFLECT);
                 if (tiled)
-                    le = launch_reflect_tile(g, sh, c->words32, tab, j0, B, slab, tl, as<int>(c->order), acc, err,
-                                             st);
+                    le = launch_reflect_tile(B, slab, tl, as<int>(c->order), acc, err, st);
                 else if (o->group_size > 0)
-                    le = launch_reflect_group(g, N, sh, c->words32, tab, j0, B, slab, gl, as<int>(c->order), acc, st);
+                    le = launch_reflect_group(N, B, slab, gl, as<int>(c->order), acc, st);
                 else
                     le = launch_reflect_block(g, N, T, sh, c->words32, tab, j0, B, slab, nl, acc,
                                               as<int>(c->order), err, st);
@@ -620,6 +636,7 @@ int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const sola
     c->timed = false;
     c->ktime = o->time_kernels != 0;
     c->group_entries = 0;
+    c->staged_rows = 0;
     c->kt_used = 0;
     c->kt_ids.clear();
     c->kt_stream = st;
@@ -710,7 +727,7 @@ int solar_gpu_create(int device, solar_gpu_context** out)
     return SOLAR_GPU_OK;
 }
 
-static constexpr int kNumBufs = 53;
+static constexpr int kNumBufs = 54;
 
 static void all_bufs(solar_gpu_context* c, DevBuf** out)
 {
@@ -722,7 +739,8 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                       &c->order_cnt, &c->order_cur, &c->order_tmp, &c->grp_cnt, &c->grp_off,
                       &c->grp_tmp, &c->grp_cell, &c->grp_w, &c->w_cnt, &c->w_off, &c->w_tmp,
                       &c->w_cell, &c->w_val, &c->order_first, &c->order_inv,
-                                &c->tile_flag, &c->tile_pos, &c->tile_start, &c->tile_union, &c->tile_slot};
+                                &c->tile_flag, &c->tile_pos, &c->tile_start, &c->tile_union, &c->tile_slot,
+                                &c->tile_rows};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 
@@ -856,6 +874,8 @@ int solar_gpu_last_timings(solar_gpu_context* c, double* ms, int n)
 long long solar_gpu_last_launch_count(solar_gpu_context* c) { return c ? c->launches : -1; }
 
 long long solar_gpu_last_reflection_entries(solar_gpu_context* c) { return c ? c->group_entries : -1; }
+
+long long solar_gpu_last_staged_rows(solar_gpu_context* c) { return c ? c->staged_rows : -1; }
 
 int solar_gpu_kernel_times(solar_gpu_context* c, double* ms, long long* launches, int n)
 {

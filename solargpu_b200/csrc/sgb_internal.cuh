@@ -152,9 +152,9 @@ cudaError_t launch_weight_lists(int pass, const DevGeom& g, int N, int T, const 
 cudaError_t launch_group_merge(int pass, int V, int N, const long long* woff, const int* wcell,
                                const float* wts, int* counts, const long long* goff, int* cell, float* w,
                                cudaStream_t st);
-cudaError_t launch_reflect_group(const DevGeom& g, int N, const uint32_t* shadow, int words32,
-                                 const HourEntry* table, int j0, int B, const float* slab,
-                                 const GroupLists& gl, const int* order, const Accum& acc, cudaStream_t st);
+// slab: [N][B] rows of every voxel (neighbor values and each voxel's own term).
+cudaError_t launch_reflect_group(int N, int B, const float* slab, const GroupLists& gl, const int* order,
+                                 const Accum& acc, cudaStream_t st);
 cudaError_t launch_finalize_f64(const double* in, int N, float* out, cudaStream_t st);
 
 // tiled reflection (tile.cu)
@@ -171,11 +171,12 @@ struct TileLists {
 // Group boundaries: flag/pos scratch [N] / [N + 1]; start [N + 1].
 cudaError_t launch_tile_groups(int N, int G, const long long* woff, int* flag, long long* pos,
                                long long* scan_tmp, int* start, cudaStream_t st);
-// Rewrites the weighted lists of each group in place into union + slots.
+// Rewrites the weighted lists of each group in place into union + slots;
+// rows_total = sum of the unions (slab rows staged per hour block).
 cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, float* wts,
-                              unsigned short* slots, int* unions, int* err, cudaStream_t st);
-cudaError_t launch_reflect_tile(const DevGeom& g, const uint32_t* shadow, int words32, const HourEntry* table,
-                                int j0, int B, const float* slab, const TileLists& tl, const int* order,
-                                const Accum& acc, int* err, cudaStream_t st);
+                              unsigned short* slots, int* unions, long long* rows_total, int* err, cudaStream_t st);
+// slab: [N][B] rows of every voxel (neighbor values and each voxel's own term).
+cudaError_t launch_reflect_tile(int B, const float* slab, const TileLists& tl, const int* order, const Accum& acc,
+                                int* err, cudaStream_t st);
 
 }  // namespace sgb

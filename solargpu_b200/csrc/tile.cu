@@ -130,7 +130,7 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* out, int* s_warp
 __global__ void __launch_bounds__(kBuildThreads)
 k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, int* __restrict__ cells,
              float* __restrict__ wts, unsigned short* __restrict__ slots, int* __restrict__ unions,
-             int* __restrict__ err)
+             unsigned long long* __restrict__ rows_total, int* __restrict__ err)
 {
     extern __shared__ __align__(16) uint32_t sm[];
     uint32_t* keys = sm;
@@ -201,7 +201,10 @@ k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, 
         slots[e0 + i] = (unsigned short)(keys[i] & 0xFFFFu);
         wts[e0 + i] = vals[i];
     }
-    if (threadIdx.x == 0) unions[q] = u;
+    if (threadIdx.x == 0) {
+        unions[q] = u;
+        atomicAdd(rows_total, (unsigned long long)u);
+    }
 }
 
 // ---- per hour block ----------------------------------------------------------
@@ -264,11 +267,24 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
                  : "memory");
 }
 
-__device__ __forceinline__ int tile_lane_hour(int Q, int lane, int q)
+template <int Q>
+__device__ __forceinline__ void global_row(float (&x)[Q], const float* __restrict__ row, int lane)
 {
-    return Q <= 4 ? lane * Q + q : 128 * (q >> 2) + 4 * lane + (q & 3);
+    if constexpr (Q == 1) {
+        x[0] = __ldg(row + lane);
+    } else if constexpr (Q == 2) {
+        const float2 a = __ldg(reinterpret_cast<const float2*>(row) + lane);
+        x[0] = a.x; x[1] = a.y;
+    } else {
+#pragma unroll
+        for (int h = 0; h < Q / 4; ++h) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(row) + lane + 32 * h);
+            x[4 * h] = a.x; x[4 * h + 1] = a.y; x[4 * h + 2] = a.z; x[4 * h + 3] = a.w;
+        }
+    }
 }
 
+// Same lane layout from a shared-memory row.
 template <int Q>
 __device__ __forceinline__ void smem_row(float (&x)[Q], const float* row, int lane)
 {
@@ -311,13 +327,13 @@ struct Window {
 
 template <int Q, int VPW>
 __global__ void __launch_bounds__((kConsumerWarps + 1) * 32, 1)
-k_reflect_tile(const float4* __restrict__ geo_n, const uint32_t* __restrict__ shadow, int words32,
-               const HourEntry* __restrict__ table, int j0, const float* __restrict__ slab, TileLists tl,
-               const int* __restrict__ order, Accum acc, int* __restrict__ err)
+k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restrict__ order, Accum acc,
+               int* __restrict__ err)
 {
     constexpr int kRowFloats = 32 * Q;
     constexpr int kRowBytes = kRowFloats * 4;
     constexpr int R = kStageBytes / kRowBytes;   // union rows per stage
+    constexpr int kCellsPerLane = (R + 31) / 32;
     extern __shared__ __align__(128) float stage_mem[];
     __shared__ __align__(8) unsigned long long bar_full[kStages], bar_empty[kStages];
     __shared__ volatile int s_abort;
@@ -342,17 +358,26 @@ k_reflect_tile(const float4* __restrict__ geo_n, const uint32_t* __restrict__ sh
             const int u = tl.unions[q];
             for (int c0 = 0; c0 < u && ok; c0 += R, ++k) {
                 const int s = (int)(k % kStages);
+                const int rows = min(R, u - c0);
+                int cell[kCellsPerLane];   // loaded before the wait so the wait hides their latency
+#pragma unroll
+                for (int i = 0; i < kCellsPerLane; ++i) {
+                    const int r = lane + 32 * i;
+                    cell[i] = r < rows ? __ldg(tl.cells + ubase + c0 + r) : 0;
+                }
                 if (k >= kStages)
                     ok = mbar_wait(smem_u32(&bar_empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_abort);
                 if (!ok) break;
-                const int rows = min(R, u - c0);
                 const unsigned full = smem_u32(&bar_full[s]);
                 if (lane == 0) mbar_expect(full, (unsigned)(rows * kRowBytes));
                 __syncwarp();
                 const unsigned dst = smem_u32(stage_mem) + (unsigned)(s * kStageBytes);
-                for (int r = lane; r < rows; r += 32) {
-                    const int g = __ldg(tl.cells + ubase + c0 + r);
-                    bulk_g2s(dst + (unsigned)(r * kRowBytes), slab + (size_t)g * kRowFloats, kRowBytes, full);
+#pragma unroll
+                for (int i = 0; i < kCellsPerLane; ++i) {
+                    const int r = lane + 32 * i;
+                    if (r < rows)
+                        bulk_g2s(dst + (unsigned)(r * kRowBytes), slab + (size_t)cell[i] * kRowFloats, kRowBytes,
+                                 full);
                 }
             }
         }
@@ -445,14 +470,13 @@ k_reflect_tile(const float4* __restrict__ geo_n, const uint32_t* __restrict__ sh
         for (int t = 0; t < VPW; ++t) {
             const int p = p0 + warp + kConsumerWarps * t;
             if (p < p1) {
+                // the voxel's own direct + diffuse is its own slab row
                 const int v = __ldg(order + p);
-                const float4 n4 = __ldg(geo_n + v);
+                float own[Q];
+                global_row<Q>(own, slab + (size_t)v * kRowFloats, lane);
                 float sum = 0.0f;
 #pragma unroll
-                for (int h = 0; h < Q; ++h) {
-                    const HourEntry e = table[j0 + tile_lane_hour(Q, lane, h)];
-                    sum += solar_I(n4, e, shadow_bit(shadow, words32, v, e.dense)) + a[t][h];
-                }
+                for (int h = 0; h < Q; ++h) sum += own[h] + a[t][h];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
                 if (lane == 0) tile_accumulate(acc, v, sum);
@@ -474,8 +498,7 @@ int tile_sms()
 }
 
 template <int Q, int VPW>
-cudaError_t tile_q(const DevGeom& g, const uint32_t* shadow, int words32, const HourEntry* table, int j0,
-                   const float* slab, const TileLists& tl, const int* order, const Accum& acc, int* err,
+cudaError_t tile_q(const float* slab, const TileLists& tl, const int* order, const Accum& acc, int* err,
                    cudaStream_t st)
 {
     const size_t smem = (size_t)kStages * kStageBytes;
@@ -490,8 +513,7 @@ cudaError_t tile_q(const DevGeom& g, const uint32_t* shadow, int words32, const 
         attr[dev] = true;
     }
     const int grid = tl.NG < tile_sms() ? tl.NG : tile_sms();
-    k_reflect_tile<Q, VPW><<<grid, (kConsumerWarps + 1) * 32, smem, st>>>(g.geo_n, shadow, words32, table, j0,
-                                                                          slab, tl, order, acc, err);
+    k_reflect_tile<Q, VPW><<<grid, (kConsumerWarps + 1) * 32, smem, st>>>(slab, tl, order, acc, err);
     return cudaGetLastError();
 }
 
@@ -512,7 +534,7 @@ cudaError_t launch_tile_groups(int N, int G, const long long* woff, int* flag, l
 }
 
 cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, float* wts,
-                              unsigned short* slots, int* unions, int* err, cudaStream_t st)
+                              unsigned short* slots, int* unions, long long* rows_total, int* err, cudaStream_t st)
 {
     if (NG <= 0) return cudaSuccess;
     const size_t smem = (size_t)3 * kTileCap * 4;
@@ -526,21 +548,23 @@ cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, i
         if (e != cudaSuccess) return e;
         attr[dev] = true;
     }
-    k_tile_build<<<NG, kBuildThreads, smem, st>>>(start, woff, cells, wts, slots, unions, err);
+    cudaError_t e = cudaMemsetAsync(rows_total, 0, sizeof(long long), st);
+    if (e != cudaSuccess) return e;
+    k_tile_build<<<NG, kBuildThreads, smem, st>>>(start, woff, cells, wts, slots, unions,
+                                                  reinterpret_cast<unsigned long long*>(rows_total), err);
     return cudaGetLastError();
 }
 
-cudaError_t launch_reflect_tile(const DevGeom& g, const uint32_t* shadow, int words32, const HourEntry* table,
-                                int j0, int B, const float* slab, const TileLists& tl, const int* order,
-                                const Accum& acc, int* err, cudaStream_t st)
+cudaError_t launch_reflect_tile(int B, const float* slab, const TileLists& tl, const int* order, const Accum& acc,
+                                int* err, cudaStream_t st)
 {
     if (tl.NG <= 0) return cudaSuccess;
     const int vpw = tl.G / kConsumerWarps;
     if (vpw == 4) {
         switch (B) {
-        case 64: return tile_q<2, 4>(g, shadow, words32, table, j0, slab, tl, order, acc, err, st);
-        case 128: return tile_q<4, 4>(g, shadow, words32, table, j0, slab, tl, order, acc, err, st);
-        case 256: return tile_q<8, 4>(g, shadow, words32, table, j0, slab, tl, order, acc, err, st);
+        case 64: return tile_q<2, 4>(slab, tl, order, acc, err, st);
+        case 128: return tile_q<4, 4>(slab, tl, order, acc, err, st);
+        case 256: return tile_q<8, 4>(slab, tl, order, acc, err, st);
         default: return cudaErrorInvalidValue;
         }
     }
