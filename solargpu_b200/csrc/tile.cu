@@ -37,8 +37,8 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kTileCap = 16384;             // entries of one group held by the build
 constexpr int kBuildThreads = 512;
 constexpr int kConsumerWarps = 16;
-constexpr int kStages = 4;
-constexpr int kStageBytes = 48 * 1024;
+constexpr int kStages = 3;
+constexpr int kStageBytes = 72 * 1024;
 constexpr unsigned long long kWaitNs = 1000000000ull;   // 1 s
 constexpr int kMaxDevices = 64;
 
@@ -96,48 +96,22 @@ __device__ __forceinline__ void block_bitonic(uint32_t* keys, float* vals, int n
     }
 }
 
-// Exclusive block scan of one int per thread; returns the total.
-__device__ __forceinline__ int block_exclusive_scan(int x, int* out, int* s_warp)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    int inc = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(kFull, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) s_warp[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        int w = lane < nw ? s_warp[lane] : 0;
-        int wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(kFull, wi, o);
-            if (lane >= o) wi += y;
-        }
-        if (lane < nw) s_warp[lane] = wi - w;
-        if (lane == 31) s_warp[32] = wi;
-    }
-    __syncthreads();
-    *out = s_warp[warp] + inc - x;
-    const int total = s_warp[32];
-    __syncthreads();
-    return total;
-}
-
-// One CTA per group.  Shared memory: keys, union and values, kTileCap each.
+// One CTA per group.  Shared memory: a hash set of the group's cells
+// (2 x kTileCap slots, load <= 1/2), reused afterwards for the (voxel, slot)
+// keys and weights; the union (kTileCap).
 __global__ void __launch_bounds__(kBuildThreads)
 k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, int* __restrict__ cells,
              float* __restrict__ wts, unsigned short* __restrict__ slots, int* __restrict__ unions,
              unsigned long long* __restrict__ rows_total, int* __restrict__ err)
 {
+    constexpr int kHashSlots = 2 * kTileCap;
     extern __shared__ __align__(16) uint32_t sm[];
-    uint32_t* keys = sm;
-    int* uni = reinterpret_cast<int*>(sm + kTileCap);
-    float* vals = reinterpret_cast<float*>(sm + 2 * kTileCap);
-    __shared__ int s_warp[33];
+    uint32_t* table = sm;                                     // [kHashSlots], key = cell + 1, 0 = empty
+    uint32_t* keys = sm;                                      // [kTileCap] after the union is built
+    float* vals = reinterpret_cast<float*>(sm + kTileCap);    // [kTileCap]
+    uint32_t* uni = sm + kHashSlots;                          // [kTileCap]
     __shared__ int s_off[257];
+    __shared__ int s_count;
     const int q = blockIdx.x;
     const int p0 = start[q], p1 = start[q + 1];
     const int nv = p1 - p0;
@@ -152,24 +126,38 @@ k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, 
     }
     const int n = (int)nl;
     for (int j = threadIdx.x; j <= nv; j += blockDim.x) s_off[j] = (int)(woff[p0 + j] - e0);
-    int n2 = kBuildThreads;
-    while (n2 < n) n2 <<= 1;
-    for (int i = threadIdx.x; i < n2; i += blockDim.x) keys[i] = i < n ? (uint32_t)cells[e0 + i] + 1u : 0u;
+    for (int i = threadIdx.x; i < kHashSlots; i += blockDim.x) table[i] = 0u;
+    if (threadIdx.x == 0) s_count = 0;
     __syncthreads();
-    block_bitonic(keys, nullptr, n2, true);
 
-    // union = distinct keys (descending), each thread compacting a contiguous range
-    const int per = n2 / kBuildThreads;
-    const int i0 = threadIdx.x * per;
-    int heads = 0;
-    for (int i = i0; i < i0 + per; ++i) heads += (i < n && (i == 0 || keys[i] != keys[i - 1])) ? 1 : 0;
-    int base = 0;
-    const int u = block_exclusive_scan(heads, &base, s_warp);
-    for (int i = i0; i < i0 + per; ++i)
-        if (i < n && (i == 0 || keys[i] != keys[i - 1])) uni[base++] = (int)keys[i] - 1;
+    // distinct cells: linear-probing insert; the inserting thread appends
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t key = (uint32_t)cells[e0 + i] + 1u;
+        uint32_t h = (key * 2654435761u) >> 17;   // 15 bits: kHashSlots = 32768
+        for (int probe = 0; probe < kHashSlots; ++probe) {
+            const uint32_t prev = atomicCAS(&table[h], 0u, key);
+            if (prev == 0u) {
+                uni[atomicAdd(&s_count, 1)] = key;
+                break;
+            }
+            if (prev == key) break;
+            h = (h + 1u) & (kHashSlots - 1);
+        }
+    }
+    __syncthreads();
+    const int u = s_count;
+    int u2 = 64;
+    while (u2 < u) u2 <<= 1;
+    for (int i = u + threadIdx.x; i < u2; i += blockDim.x) uni[i] = 0u;
+    __syncthreads();
+    block_bitonic(uni, nullptr, u2, true);   // descending cell order
+    int* ucell = reinterpret_cast<int*>(uni);
+    for (int i = threadIdx.x; i < u; i += blockDim.x) ucell[i] = (int)uni[i] - 1;
     __syncthreads();
 
     // entries -> (local voxel << 16 | slot), weights alongside
+    int n2 = kBuildThreads;
+    while (n2 < n) n2 <<= 1;
     bool unsorted = false;
     for (int i = threadIdx.x; i < n2; i += blockDim.x) {
         uint32_t k = 0xFFFFFFFFu;
@@ -179,7 +167,7 @@ k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, 
             int lo = 0, hi = u - 1;
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
-                if (uni[mid] > cell) lo = mid + 1; else hi = mid;
+                if (ucell[mid] > cell) lo = mid + 1; else hi = mid;
             }
             int a = 0, b = nv;   // largest j with s_off[j] <= i
             while (b - a > 1) {
@@ -196,7 +184,7 @@ k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, 
     for (int i = threadIdx.x + 1; i < n; i += blockDim.x) unsorted |= keys[i] < keys[i - 1];
     if (__syncthreads_or(unsorted)) block_bitonic(keys, vals, n2, false);
 
-    for (int i = threadIdx.x; i < u; i += blockDim.x) cells[e0 + i] = uni[i];
+    for (int i = threadIdx.x; i < u; i += blockDim.x) cells[e0 + i] = ucell[i];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         slots[e0 + i] = (unsigned short)(keys[i] & 0xFFFFu);
         wts[e0 + i] = vals[i];
