@@ -83,7 +83,8 @@ struct solar_gpu_context {
         acc_f64, acc_f32, acc_comp, sums, out_f64, err, in_grid, in_pp, in_wz, in_slopes,
         in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
-        tile_start, tile_union, tile_slot, tile_rows;
+        tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
+        tile_erow, tile_ew;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
@@ -513,7 +514,9 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 gl.weights = as<float>(c->w_val);
             } else if (tiled) {
                 // Groups of up to V visiting positions; the weighted lists of
-                // each group are rewritten in place into union cells + slots.
+                // each group are rewritten in place into union cells + slots,
+                // then the slot lists of each 4 consecutive voxels are merged
+                // and laid out chunk by chunk.
                 RK(ensure(c->tile_flag, sizeof(int) * (size_t)N));
                 RK(ensure(c->tile_pos, sizeof(long long) * ((size_t)N + 1)));
                 RK(ensure(c->tile_start, sizeof(int) * ((size_t)N + 1)));
@@ -536,16 +539,51 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                                          as<long long>(c->tile_rows), err, st));
                 }
                 RK(read_ll(c, as<long long>(c->tile_rows), &c->staged_rows, st));
-                c->launches += 5;
-                c->group_entries = Ew;
+                const int R = tile_rows_per_stage(B);
+                RK(ensure(c->tile_gcnt, sizeof(int) * (size_t)NG));
+                RK(ensure(c->tile_gnch, sizeof(int) * (size_t)NG));
+                RK(ensure(c->tile_gbase, sizeof(long long) * ((size_t)NG + 1)));
+                RK(ensure(c->tile_tbase, sizeof(long long) * ((size_t)NG + 1)));
+                {
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(launch_tile_layout(0, (int)NG, R, as<int>(c->tile_start), as<int>(c->tile_union),
+                                          as<long long>(c->w_off), as<unsigned short>(c->tile_slot),
+                                          as<float>(c->w_val), as<int>(c->tile_gcnt), as<int>(c->tile_gnch),
+                                          nullptr, nullptr, nullptr, nullptr, nullptr, st));
+                    CK(launch_scan_counts(as<int>(c->tile_gcnt), (int)NG, 0, as<long long>(c->tile_gbase),
+                                          as<long long>(c->w_tmp), nullptr, st));
+                    CK(launch_scan_counts(as<int>(c->tile_gnch), (int)NG, 0, as<long long>(c->tile_tbase),
+                                          as<long long>(c->w_tmp), nullptr, st));
+                }
+                long long Em = 0, TC = 0;
+                RK(read_ll(c, as<long long>(c->tile_gbase) + NG, &Em, st));
+                RK(read_ll(c, as<long long>(c->tile_tbase) + NG, &TC, st));
+                RK(ensure(c->tile_erow, sizeof(unsigned short) * (size_t)(Em + 8)));
+                RK(ensure(c->tile_ew, sizeof(float4) * (size_t)(Em + 8)));
+                RK(ensure(c->tile_table, sizeof(int) * 20 * (size_t)(TC + 1)));
+                {
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(cudaMemsetAsync(c->tile_ew.p, 0, sizeof(float4) * (size_t)(Em + 8), st));
+                    CK(launch_tile_layout(1, (int)NG, R, as<int>(c->tile_start), as<int>(c->tile_union),
+                                          as<long long>(c->w_off), as<unsigned short>(c->tile_slot),
+                                          as<float>(c->w_val), nullptr, nullptr, as<long long>(c->tile_gbase),
+                                          as<long long>(c->tile_tbase), as<int>(c->tile_table),
+                                          as<unsigned short>(c->tile_erow), as<float4>(c->tile_ew), st));
+                }
+                c->launches += 10;
+                c->group_entries = Em;
                 tl.G = V;
                 tl.NG = (int)NG;
                 tl.start = as<int>(c->tile_start);
                 tl.unions = as<int>(c->tile_union);
                 tl.woff = as<long long>(c->w_off);
                 tl.cells = as<int>(c->w_cell);
-                tl.slots = as<unsigned short>(c->tile_slot);
-                tl.weights = as<float>(c->w_val);
+                tl.R = R;
+                tl.gbase = as<long long>(c->tile_gbase);
+                tl.tbase = as<long long>(c->tile_tbase);
+                tl.table = as<int>(c->tile_table);
+                tl.erow = as<unsigned short>(c->tile_erow);
+                tl.ew = as<float4>(c->tile_ew);
             } else {
                 const int G = group_count(N, V);
                 RK(ensure(c->grp_cnt, sizeof(int) * (size_t)G));
@@ -727,7 +765,7 @@ int solar_gpu_create(int device, solar_gpu_context** out)
     return SOLAR_GPU_OK;
 }
 
-static constexpr int kNumBufs = 54;
+static constexpr int kNumBufs = 61;
 
 static void all_bufs(solar_gpu_context* c, DevBuf** out)
 {
@@ -740,7 +778,8 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                       &c->grp_tmp, &c->grp_cell, &c->grp_w, &c->w_cnt, &c->w_off, &c->w_tmp,
                       &c->w_cell, &c->w_val, &c->order_first, &c->order_inv,
                                 &c->tile_flag, &c->tile_pos, &c->tile_start, &c->tile_union, &c->tile_slot,
-                                &c->tile_rows};
+                                &c->tile_rows, &c->tile_gcnt, &c->tile_gnch, &c->tile_gbase, &c->tile_tbase,
+                                &c->tile_table, &c->tile_erow, &c->tile_ew};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

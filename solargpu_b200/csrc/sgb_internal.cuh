@@ -159,22 +159,35 @@ cudaError_t launch_finalize_f64(const double* in, int N, float* out, cudaStream_
 
 // tiled reflection (tile.cu)
 struct TileLists {
-    int G;                         // voxels per group at most (64)
+    int G;                         // voxels per group at most (64 = 16 quads)
     int NG;                        // groups
     const int* start;              // [NG + 1] first visiting position of each group
     const int* unions;             // [NG] union rows of each group
     const long long* woff;         // [N + 1] entry offsets per visiting position
     const int* cells;              // union cells of group q at woff[start[q]] (descending)
-    const unsigned short* slots;   // [E] union index of each entry, ascending per voxel
-    const float* weights;          // [E] weight of each entry
+    int R;                         // union rows per chunk (rows one shared-memory stage holds)
+    const long long* gbase;        // [NG + 1] first merged entry of each group
+    const long long* tbase;        // [NG + 1] first chunk table of each group
+    const int* table;              // [chunks][20] per chunk: quad offsets, block start, padded count
+    const unsigned short* erow;    // [Em] row of each merged entry inside its chunk
+    const float4* ew;              // [Em] the quad's 4 weights for that row (0 where a voxel lacks it)
 };
 // Group boundaries: flag/pos scratch [N] / [N + 1]; start [N + 1].
 cudaError_t launch_tile_groups(int N, int G, const long long* woff, int* flag, long long* pos,
                                long long* scan_tmp, int* start, cudaStream_t st);
+// Union rows per chunk of the tile kernel for hour block B (0 if not built).
+int tile_rows_per_stage(int B);
 // Rewrites the weighted lists of each group in place into union + slots;
 // rows_total = sum of the unions (slab rows staged per hour block).
 cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, float* wts,
                               unsigned short* slots, int* unions, long long* rows_total, int* err, cudaStream_t st);
+// Merges the slot lists of each quad and lays them out chunk by chunk:
+// pass 0 counts (gcnt: padded merged entries, gnch: chunks, per group),
+// pass 1 writes at gbase / tbase (scans of gcnt / gnch); ew must be zero.
+cudaError_t launch_tile_layout(int pass, int NG, int R, const int* start, const int* unions, const long long* woff,
+                               const unsigned short* slots, const float* wts, int* gcnt, int* gnch,
+                               const long long* gbase, const long long* tbase, int* table,
+                               unsigned short* erow, float4* ew, cudaStream_t st);
 // slab: [N][B] rows of every voxel (neighbor values and each voxel's own term).
 cudaError_t launch_reflect_tile(int B, const float* slab, const TileLists& tl, const int* order, const Accum& acc,
                                 int* err, cudaStream_t st);

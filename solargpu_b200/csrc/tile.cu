@@ -37,10 +37,11 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kTileCap = 16384;             // entries of one group held by the build
 constexpr int kBuildThreads = 512;
 constexpr int kConsumerWarps = 16;
+constexpr int kProducerWarps = 4;            // 20 warps: 5 a sub-partition, 96 registers a thread
 constexpr int kStages = 3;
-constexpr int kStageBytes = 72 * 1024;
 constexpr unsigned long long kWaitNs = 1000000000ull;   // 1 s
 constexpr int kMaxDevices = 64;
+constexpr int kQuad = 4;                    // voxels merged per consumer warp
 
 // ---- grouping ----------------------------------------------------------------
 
@@ -195,6 +196,156 @@ k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, 
     }
 }
 
+// ---- layout: merged quads, chunk-major -------------------------------------
+//
+// Consumer warp w of a group owns the quad of positions p0 + 4w .. p0 + 4w + 3.
+// The slot lists of a quad's 4 voxels are merged (one entry per distinct
+// slot, the 4 weights alongside, 0 where a voxel lacks the slot), and the
+// group's merged entries are laid out chunk by chunk (chunk c = slots
+// [cR, cR + R), the rows one stage holds), quads in order inside a chunk,
+// slots ascending inside a quad.  Each chunk's block is padded to a multiple
+// of 8 entries so that it can be bulk-copied (16-byte sizes and addresses).
+// Per chunk a table of kTabInts ints: [0..16] = exclusive offsets of the 16
+// quads inside the block (tab[16] = entries), [17] = block start relative to
+// the group's first entry, [18] = padded entry count.
+//
+// One CTA per group, one warp per quad.  A bitmap over the union slots marks
+// the quad's slots; ranks come from prefix popcounts.  PASS 0 counts (padded
+// entries and chunks per group), PASS 1 writes at the scanned offsets; ew
+// must be zero beforehand.
+
+constexpr int kTabInts = 20;
+constexpr int kMaxChunks = kTileCap / 32 + 1;   // R >= 32
+
+__device__ __forceinline__ int bit_rank(const uint32_t* bits, const int* pre, int x)
+{
+    return pre[x >> 5] + __popc(bits[x >> 5] & ((1u << (x & 31)) - 1u));
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(kConsumerWarps * 32)
+k_tile_layout(int R, const int* __restrict__ start, const int* __restrict__ unions,
+              const long long* __restrict__ woff, const unsigned short* __restrict__ slots,
+              const float* __restrict__ wts, int* __restrict__ gcnt, int* __restrict__ gnch,
+              const long long* __restrict__ gbase, const long long* __restrict__ tbase, int* __restrict__ table,
+              unsigned short* __restrict__ erow, float4* __restrict__ ew)
+{
+    constexpr int kWords = kTileCap / 32;
+    extern __shared__ __align__(16) uint32_t lsm[];
+    uint32_t* s_bits = lsm;                                                     // [16][kWords + 1]
+    int* s_pre = reinterpret_cast<int*>(lsm + kConsumerWarps * (kWords + 1));   // [16][kWords + 1]
+    int* s_cw = s_pre + kConsumerWarps * (kWords + 1);                          // [kMaxChunks][17]
+    int* s_cs = s_cw + kMaxChunks * 17;                                         // [kMaxChunks + 1]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x;
+    const int p0 = start[q], p1 = start[q + 1];
+    const int u = unions[q];
+    const int words = (u + 31) >> 5;
+    const int nch = (u + R - 1) / R;
+    uint32_t* bits = s_bits + warp * (kWords + 1);
+    int* pre = s_pre + warp * (kWords + 1);
+    const int lead = p0 + kQuad * warp;
+    const int n = lead < p1 ? min(kQuad, p1 - lead) : 0;
+    for (int w = lane; w <= words; w += 32) bits[w] = 0u;
+    __syncwarp();
+    long long e0 = 0, e1 = 0, b1 = 0, b2 = 0, b3 = 0;
+    if (n > 0) {
+        e0 = woff[lead];
+        e1 = woff[lead + n];
+        b1 = woff[lead + 1];
+        b2 = n > 2 ? woff[lead + 2] : e1;
+        b3 = n > 3 ? woff[lead + 3] : e1;
+        for (long long i = e0 + lane; i < e1; i += 32) {
+            const int sl = slots[i];
+            atomicOr(&bits[sl >> 5], 1u << (sl & 31));
+        }
+    }
+    __syncwarp();
+    int carry = 0;
+    for (int w0 = 0; w0 <= words; w0 += 32) {
+        const int w = w0 + lane;
+        const int c = w < words ? __popc(bits[w]) : 0;
+        int inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (w <= words) pre[w] = carry + inc - c;
+        carry += __shfl_sync(kFull, inc, 31);
+    }
+    __syncwarp();
+    // entries of this quad per chunk
+    for (int c = lane; c < nch; c += 32) {
+        const int lo = c * R, hi = min(lo + R, u);
+        s_cw[c * 17 + warp] = bit_rank(bits, pre, hi) - bit_rank(bits, pre, lo);
+    }
+    __syncthreads();
+    // per chunk: exclusive offsets over quads, padded block sizes
+    for (int c = threadIdx.x; c < nch; c += blockDim.x) {
+        int acc = 0;
+        for (int w = 0; w < kConsumerWarps; ++w) {
+            const int x = s_cw[c * 17 + w];
+            s_cw[c * 17 + w] = acc;
+            acc += x;
+        }
+        s_cw[c * 17 + 16] = acc;
+        s_cs[c] = (acc + 7) & ~7;
+    }
+    __syncthreads();
+    if (warp == 0) {   // exclusive scan of the padded block sizes
+        int run = 0;
+        for (int c0 = 0; c0 < nch; c0 += 32) {
+            const int c = c0 + lane;
+            const int x = c < nch ? s_cs[c] : 0;
+            int inc = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, inc, o);
+                if (lane >= o) inc += y;
+            }
+            __syncwarp();
+            if (c < nch) s_cs[c] = run + inc - x;
+            run += __shfl_sync(kFull, inc, 31);
+        }
+        if (lane == 0) s_cs[nch] = run;
+    }
+    __syncthreads();
+    if (PASS == 0) {
+        if (threadIdx.x == 0) {
+            gcnt[q] = s_cs[nch];
+            gnch[q] = nch;
+        }
+        return;
+    }
+    const long long gb = gbase[q];
+    int* tab = table + tbase[q] * kTabInts;
+    for (int i = threadIdx.x; i < nch * kTabInts; i += blockDim.x) {
+        const int c = i / kTabInts, k = i % kTabInts;
+        int v = 0;
+        if (k <= 16) v = s_cw[c * 17 + k];
+        else if (k == 17) v = s_cs[c];
+        else if (k == 18) v = s_cs[c + 1] - s_cs[c];
+        tab[i] = v;
+    }
+    if (n > 0) {
+        for (long long i = e0 + lane; i < e1; i += 32) {
+            const int sl = slots[i];
+            const int c = sl / R;
+            const long long d = gb + s_cs[c] + s_cw[c * 17 + warp] + bit_rank(bits, pre, sl) -
+                                bit_rank(bits, pre, c * R);
+            const int t = (i >= b1) + (i >= b2) + (i >= b3);
+            erow[d] = (unsigned short)(sl - c * R);
+            reinterpret_cast<float*>(ew + d)[t] = wts[i];
+        }
+    }
+}
+
+size_t layout_smem()
+{
+    return sizeof(uint32_t) * (size_t)(2 * kConsumerWarps * (kTileCap / 32 + 1) + kMaxChunks * 17 + kMaxChunks + 1);
+}
+
 // ---- per hour block ----------------------------------------------------------
 
 __device__ __forceinline__ unsigned smem_u32(const void* p)
@@ -305,24 +456,32 @@ __device__ __forceinline__ void tile_accumulate(const Accum& a, int v, float x)
     }
 }
 
-// Entry window of one voxel, relative to the group's first entry: lane l
-// holds entry wbase + l.
-struct Window {
-    int e, end, wbase;
-    int slot;
-    float w;
+// One stage of the ring: R union rows, then the chunk's entry block (4
+// weights, row index) and its quad table.
+template <int Q>
+struct StageLayout {
+    static constexpr int kRowBytes = 32 * Q * 4;
+    static constexpr int kBudget = 72 * 1024;
+    static constexpr int R = ((kBudget - kTabInts * 4) / (kRowBytes + kConsumerWarps * 18)) & ~7;
+    static constexpr int kMaxEntries = kConsumerWarps * R;   // one entry per quad and row at most
+    static constexpr int kW = R * kRowBytes;                  // float4 weights
+    static constexpr int kRow = kW + kMaxEntries * 16;         // u16 row indices
+    static constexpr int kTab = kRow + kMaxEntries * 2;        // table
+    static constexpr int kBytes = kTab + kTabInts * 4;
+    static_assert(kW % 16 == 0 && kRow % 16 == 0 && kTab % 16 == 0 && kBytes % 16 == 0, "16-byte stage parts");
 };
 
-template <int Q, int VPW>
-__global__ void __launch_bounds__((kConsumerWarps + 1) * 32, 1)
+template <int Q>
+__global__ void __launch_bounds__((kConsumerWarps + kProducerWarps) * 32, 1)
 k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restrict__ order, Accum acc,
                int* __restrict__ err)
 {
+    using L = StageLayout<Q>;
     constexpr int kRowFloats = 32 * Q;
-    constexpr int kRowBytes = kRowFloats * 4;
-    constexpr int R = kStageBytes / kRowBytes;   // union rows per stage
-    constexpr int kCellsPerLane = (R + 31) / 32;
-    extern __shared__ __align__(128) float stage_mem[];
+    constexpr int kRowBytes = L::kRowBytes;
+    constexpr int R = L::R;
+    static_assert(R <= kProducerWarps * 32, "one union row per producer thread");
+    extern __shared__ __align__(128) unsigned char stage_mem[];
     __shared__ __align__(8) unsigned long long bar_full[kStages], bar_empty[kStages];
     __shared__ volatile int s_abort;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -337,43 +496,45 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
     }
     __syncthreads();
 
-    if (warp == kConsumerWarps) {
-        // ---- producer: union rows of each group into the stage ring
+    if (warp >= kConsumerWarps) {
+        // ---- producer: per chunk, the union rows, the entry block and its table
         long long k = 0;   // chunks issued by this CTA
         bool ok = true;
         for (int q = blockIdx.x; q < tl.NG && ok; q += gridDim.x) {
             const long long ubase = tl.woff[tl.start[q]];
+            const long long gb = tl.gbase[q];
+            const int* tab = tl.table + tl.tbase[q] * kTabInts;
             const int u = tl.unions[q];
-            for (int c0 = 0; c0 < u && ok; c0 += R, ++k) {
+            for (int c0 = 0, c = 0; c0 < u && ok; c0 += R, ++c, ++k) {
                 const int s = (int)(k % kStages);
                 const int rows = min(R, u - c0);
-                int cell[kCellsPerLane];   // loaded before the wait so the wait hides their latency
-#pragma unroll
-                for (int i = 0; i < kCellsPerLane; ++i) {
-                    const int r = lane + 32 * i;
-                    cell[i] = r < rows ? __ldg(tl.cells + ubase + c0 + r) : 0;
-                }
+                const int r = (warp - kConsumerWarps) * 32 + lane;   // this thread's row
+                // loaded before the wait so that the wait hides their latency
+                const int cell = r < rows ? __ldg(tl.cells + ubase + c0 + r) : 0;
+                const int bstart = __ldg(tab + c * kTabInts + 17);
+                const int bcount = __ldg(tab + c * kTabInts + 18);
                 if (k >= kStages)
                     ok = mbar_wait(smem_u32(&bar_empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_abort);
                 if (!ok) break;
                 const unsigned full = smem_u32(&bar_full[s]);
-                if (lane == 0) mbar_expect(full, (unsigned)(rows * kRowBytes));
-                __syncwarp();
-                const unsigned dst = smem_u32(stage_mem) + (unsigned)(s * kStageBytes);
-#pragma unroll
-                for (int i = 0; i < kCellsPerLane; ++i) {
-                    const int r = lane + 32 * i;
-                    if (r < rows)
-                        bulk_g2s(dst + (unsigned)(r * kRowBytes), slab + (size_t)cell[i] * kRowFloats, kRowBytes,
-                                 full);
+                const unsigned dst = smem_u32(stage_mem) + (unsigned)(s * L::kBytes);
+                if (r == 0) {
+                    mbar_expect(full, (unsigned)(rows * kRowBytes + bcount * 18 + kTabInts * 4));
+                    bulk_g2s(dst + L::kTab, tab + c * kTabInts, kTabInts * 4, full);
+                    if (bcount > 0) {
+                        bulk_g2s(dst + L::kW, tl.ew + gb + bstart, (unsigned)(bcount * 16), full);
+                        bulk_g2s(dst + L::kRow, tl.erow + gb + bstart, (unsigned)(bcount * 2), full);
+                    }
                 }
+                if (r < rows)
+                    bulk_g2s(dst + (unsigned)(r * kRowBytes), slab + (size_t)cell * kRowFloats, kRowBytes, full);
             }
         }
         if (!ok) {
             if (lane == 0) atomicOr(err, kErrWaitTimeout);
             s_abort = 1;
         }
-        // let this CTA's copies land before it exits
+        // let the copies of this warp (and the CTA) land before it exits
         if (lane == 0) {
             for (long long j = (k > kStages ? k - kStages : 0); j < k; ++j)
                 mbar_wait(smem_u32(&bar_full[j % kStages]), (unsigned)((j / kStages) & 1), nullptr);
@@ -381,28 +542,17 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
         return;
     }
 
-    // ---- consumers
+    // ---- consumers: warp w owns the quad of positions p0 + 4w .. p0 + 4w + 3
     long long k = 0;
     for (int q = blockIdx.x; q < tl.NG; q += gridDim.x) {
         const int p0 = tl.start[q], p1 = tl.start[q + 1];
         const int u = tl.unions[q];
-        const long long gbase = tl.woff[p0];
-        const unsigned short* gslots = tl.slots + gbase;
-        const float* gw = tl.weights + gbase;
-        float a[VPW][Q];
-        Window win[VPW];
+        const int lead = p0 + kQuad * warp;
+        float a[kQuad][Q];
 #pragma unroll
-        for (int t = 0; t < VPW; ++t) {
-            const int p = p0 + warp + kConsumerWarps * t;
-            const bool has = p < p1;
-            win[t].e = has ? (int)(tl.woff[p] - gbase) : 0;
-            win[t].end = has ? (int)(tl.woff[p + 1] - gbase) : 0;
-            win[t].wbase = win[t].e - 32;   // empty window: loaded on first use
-            win[t].slot = 0x7FFFFFFF;
-            win[t].w = 0.0f;
+        for (int t = 0; t < kQuad; ++t)
 #pragma unroll
             for (int h = 0; h < Q; ++h) a[t][h] = 0.0f;
-        }
         for (int c0 = 0; c0 < u; c0 += R, ++k) {
             const int s = (int)(k % kStages);
             if (!mbar_wait(smem_u32(&bar_full[s]), (unsigned)((k / kStages) & 1), &s_abort)) {
@@ -410,53 +560,33 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
                 s_abort = 1;
                 return;
             }
-            const float* rows = stage_mem + (size_t)s * (kStageBytes / 4);
-            const int lim = c0 + R;
+            const unsigned char* st = stage_mem + (size_t)s * L::kBytes;
+            const float* rows = reinterpret_cast<const float*>(st);
+            const float4* wv = reinterpret_cast<const float4*>(st + L::kW);
+            const unsigned short* rv = reinterpret_cast<const unsigned short*>(st + L::kRow);
+            const int* tab = reinterpret_cast<const int*>(st + L::kTab);
+            const int b = tab[warp], e = tab[warp + 1];
+#pragma unroll 2
+            for (int i = b; i < e; ++i) {
+                const int r = rv[i];
+                const float4 w = wv[i];
+                float x[Q];
+                smem_row<Q>(x, rows + r * kRowFloats, lane);
 #pragma unroll
-            for (int t = 0; t < VPW; ++t) {
-                Window& W = win[t];
-                while (W.e < W.end) {
-                    if (W.e - W.wbase >= 32) {
-                        W.wbase = W.e;
-                        const int i = W.e + lane;
-                        W.slot = i < W.end ? (int)__ldg(gslots + i) : 0x7FFFFFFF;
-                        W.w = i < W.end ? __ldg(gw + i) : 0.0f;
-                    }
-                    const int m = __popc(__ballot_sync(kFull, W.slot < lim));   // sorted: a prefix
-                    const int cur = W.e - W.wbase;
-                    if (cur >= m) break;
-                    int j = cur;
-                    for (; j + 1 < m; j += 2) {
-                        const int s0 = __shfl_sync(kFull, W.slot, j) - c0;
-                        const int s1 = __shfl_sync(kFull, W.slot, j + 1) - c0;
-                        const float w0 = __shfl_sync(kFull, W.w, j);
-                        const float w1 = __shfl_sync(kFull, W.w, j + 1);
-                        float x0[Q], x1[Q];
-                        smem_row<Q>(x0, rows + (size_t)s0 * kRowFloats, lane);
-                        smem_row<Q>(x1, rows + (size_t)s1 * kRowFloats, lane);
+                for (int h = 0; h < Q; ++h) a[0][h] = fmaf(w.x, x[h], a[0][h]);
 #pragma unroll
-                        for (int h = 0; h < Q; ++h) a[t][h] = fmaf(w0, x0[h], a[t][h]);
+                for (int h = 0; h < Q; ++h) a[1][h] = fmaf(w.y, x[h], a[1][h]);
 #pragma unroll
-                        for (int h = 0; h < Q; ++h) a[t][h] = fmaf(w1, x1[h], a[t][h]);
-                    }
-                    if (j < m) {
-                        const int s0 = __shfl_sync(kFull, W.slot, j) - c0;
-                        const float w0 = __shfl_sync(kFull, W.w, j);
-                        float x0[Q];
-                        smem_row<Q>(x0, rows + (size_t)s0 * kRowFloats, lane);
+                for (int h = 0; h < Q; ++h) a[2][h] = fmaf(w.z, x[h], a[2][h]);
 #pragma unroll
-                        for (int h = 0; h < Q; ++h) a[t][h] = fmaf(w0, x0[h], a[t][h]);
-                    }
-                    W.e = W.wbase + m;
-                    if (m < 32) break;
-                }
+                for (int h = 0; h < Q; ++h) a[3][h] = fmaf(w.w, x[h], a[3][h]);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&bar_empty[s]));
         }
 #pragma unroll
-        for (int t = 0; t < VPW; ++t) {
-            const int p = p0 + warp + kConsumerWarps * t;
+        for (int t = 0; t < kQuad; ++t) {
+            const int p = lead + t;
             if (p < p1) {
                 // the voxel's own direct + diffuse is its own slab row
                 const int v = __ldg(order + p);
@@ -485,34 +615,53 @@ int tile_sms()
     return sms;
 }
 
-template <int Q, int VPW>
+// Sets the dynamic shared-memory limit of a kernel once per device.
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes, bool (&done)[kMaxDevices])
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (!done[dev]) {
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        done[dev] = true;
+    }
+    return cudaSuccess;
+}
+
+template <int Q>
 cudaError_t tile_q(const float* slab, const TileLists& tl, const int* order, const Accum& acc, int* err,
                    cudaStream_t st)
 {
-    const size_t smem = (size_t)kStages * kStageBytes;
+    if (tl.R != StageLayout<Q>::R) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)kStages * StageLayout<Q>::kBytes;
     static bool attr[kMaxDevices] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!attr[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(k_reflect_tile<Q, VPW>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr[dev] = true;
-    }
+    cudaError_t e = allow_smem(k_reflect_tile<Q>, smem, attr);
+    if (e != cudaSuccess) return e;
     const int grid = tl.NG < tile_sms() ? tl.NG : tile_sms();
-    k_reflect_tile<Q, VPW><<<grid, (kConsumerWarps + 1) * 32, smem, st>>>(slab, tl, order, acc, err);
+    k_reflect_tile<Q><<<grid, (kConsumerWarps + kProducerWarps) * 32, smem, st>>>(slab, tl, order, acc, err);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-int tile_voxels_per_warp(int G) { return G / kConsumerWarps; }
+int tile_rows_per_stage(int B)
+{
+    switch (B) {
+    case 64: return StageLayout<2>::R;
+    case 128: return StageLayout<4>::R;
+    case 256: return StageLayout<8>::R;
+    default: return 0;
+    }
+}
 
 cudaError_t launch_tile_groups(int N, int G, const long long* woff, int* flag, long long* pos,
                                long long* scan_tmp, int* start, cudaStream_t st)
 {
     if (N <= 0) return cudaSuccess;
+    if (G != kQuad * kConsumerWarps) return cudaErrorInvalidValue;
     const unsigned grid = (unsigned)((N + 255) / 256);
     k_tile_flags<<<grid, 256, 0, st>>>(N, G, woff, flag);
     cudaError_t e = launch_scan_counts(flag, N, 0, pos, scan_tmp, nullptr, st);
@@ -527,19 +676,32 @@ cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, i
     if (NG <= 0) return cudaSuccess;
     const size_t smem = (size_t)3 * kTileCap * 4;
     static bool attr[kMaxDevices] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!attr[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(k_tile_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)smem);
-        if (e != cudaSuccess) return e;
-        attr[dev] = true;
-    }
-    cudaError_t e = cudaMemsetAsync(rows_total, 0, sizeof(long long), st);
+    cudaError_t e = allow_smem(k_tile_build, smem, attr);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(rows_total, 0, sizeof(long long), st);
     if (e != cudaSuccess) return e;
     k_tile_build<<<NG, kBuildThreads, smem, st>>>(start, woff, cells, wts, slots, unions,
                                                   reinterpret_cast<unsigned long long*>(rows_total), err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_layout(int pass, int NG, int R, const int* start, const int* unions, const long long* woff,
+                               const unsigned short* slots, const float* wts, int* gcnt, int* gnch,
+                               const long long* gbase, const long long* tbase, int* table,
+                               unsigned short* erow, float4* ew, cudaStream_t st)
+{
+    if (NG <= 0) return cudaSuccess;
+    if (R < 32) return cudaErrorInvalidValue;
+    const size_t smem = layout_smem();
+    static bool attr0[kMaxDevices] = {}, attr1[kMaxDevices] = {};
+    cudaError_t e = pass == 0 ? allow_smem(k_tile_layout<0>, smem, attr0) : allow_smem(k_tile_layout<1>, smem, attr1);
+    if (e != cudaSuccess) return e;
+    if (pass == 0)
+        k_tile_layout<0><<<NG, kConsumerWarps * 32, smem, st>>>(R, start, unions, woff, slots, wts, gcnt, gnch,
+                                                                gbase, tbase, table, erow, ew);
+    else
+        k_tile_layout<1><<<NG, kConsumerWarps * 32, smem, st>>>(R, start, unions, woff, slots, wts, gcnt, gnch,
+                                                                gbase, tbase, table, erow, ew);
     return cudaGetLastError();
 }
 
@@ -547,16 +709,13 @@ cudaError_t launch_reflect_tile(int B, const float* slab, const TileLists& tl, c
                                 int* err, cudaStream_t st)
 {
     if (tl.NG <= 0) return cudaSuccess;
-    const int vpw = tl.G / kConsumerWarps;
-    if (vpw == 4) {
-        switch (B) {
-        case 64: return tile_q<2, 4>(slab, tl, order, acc, err, st);
-        case 128: return tile_q<4, 4>(slab, tl, order, acc, err, st);
-        case 256: return tile_q<8, 4>(slab, tl, order, acc, err, st);
-        default: return cudaErrorInvalidValue;
-        }
+    if (tl.G != kQuad * kConsumerWarps) return cudaErrorInvalidValue;
+    switch (B) {
+    case 64: return tile_q<2>(slab, tl, order, acc, err, st);
+    case 128: return tile_q<4>(slab, tl, order, acc, err, st);
+    case 256: return tile_q<8>(slab, tl, order, acc, err, st);
+    default: return cudaErrorInvalidValue;
     }
-    return cudaErrorInvalidValue;
 }
 
 }  // namespace sgb
