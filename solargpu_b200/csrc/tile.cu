@@ -38,7 +38,7 @@ constexpr int kTileCap = 16384;             // entries of one group held by the 
 constexpr int kBuildThreads = 512;
 constexpr int kConsumerWarps = 16;
 constexpr int kProducerWarps = 4;            // 20 warps: 5 a sub-partition, 96 registers a thread
-constexpr int kStages = 3;
+constexpr int kStages = 2;
 constexpr unsigned long long kWaitNs = 1000000000ull;   // 1 s
 constexpr int kMaxDevices = 64;
 constexpr int kQuad = 4;                    // voxels merged per consumer warp
@@ -461,7 +461,7 @@ __device__ __forceinline__ void tile_accumulate(const Accum& a, int v, float x)
 template <int Q>
 struct StageLayout {
     static constexpr int kRowBytes = 32 * Q * 4;
-    static constexpr int kBudget = 72 * 1024;
+    static constexpr int kBudget = 108 * 1024;
     static constexpr int R = ((kBudget - kTabInts * 4) / (kRowBytes + kConsumerWarps * 18)) & ~7;
     static constexpr int kMaxEntries = kConsumerWarps * R;   // one entry per quad and row at most
     static constexpr int kW = R * kRowBytes;                  // float4 weights
@@ -480,7 +480,8 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
     constexpr int kRowFloats = 32 * Q;
     constexpr int kRowBytes = L::kRowBytes;
     constexpr int R = L::R;
-    static_assert(R <= kProducerWarps * 32, "one union row per producer thread");
+    constexpr int kProducers = kProducerWarps * 32;
+    constexpr int kRowsPerThread = (R + kProducers - 1) / kProducers;
     extern __shared__ __align__(128) unsigned char stage_mem[];
     __shared__ __align__(8) unsigned long long bar_full[kStages], bar_empty[kStages];
     __shared__ volatile int s_abort;
@@ -505,20 +506,39 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
             const long long gb = tl.gbase[q];
             const int* tab = tl.table + tl.tbase[q] * kTabInts;
             const int u = tl.unions[q];
+            // this thread's rows r0 + kProducers * i of every chunk; the next
+            // chunk's cells and table entries are loaded one chunk ahead
+            const int r0 = (warp - kConsumerWarps) * 32 + lane;
+            int ncell[kRowsPerThread];
+#pragma unroll
+            for (int i = 0; i < kRowsPerThread; ++i) {
+                const int r = r0 + kProducers * i;
+                ncell[i] = r < min(R, u) ? __ldg(tl.cells + ubase + r) : 0;
+            }
+            int nbstart = u > 0 ? __ldg(tab + 17) : 0;
+            int nbcount = u > 0 ? __ldg(tab + 18) : 0;
             for (int c0 = 0, c = 0; c0 < u && ok; c0 += R, ++c, ++k) {
                 const int s = (int)(k % kStages);
                 const int rows = min(R, u - c0);
-                const int r = (warp - kConsumerWarps) * 32 + lane;   // this thread's row
-                // loaded before the wait so that the wait hides their latency
-                const int cell = r < rows ? __ldg(tl.cells + ubase + c0 + r) : 0;
-                const int bstart = __ldg(tab + c * kTabInts + 17);
-                const int bcount = __ldg(tab + c * kTabInts + 18);
+                int cell[kRowsPerThread];
+#pragma unroll
+                for (int i = 0; i < kRowsPerThread; ++i) cell[i] = ncell[i];
+                const int bstart = nbstart, bcount = nbcount;
+                if (c0 + R < u) {
+#pragma unroll
+                    for (int i = 0; i < kRowsPerThread; ++i) {
+                        const int r = r0 + kProducers * i;
+                        ncell[i] = r < min(R, u - c0 - R) ? __ldg(tl.cells + ubase + c0 + R + r) : 0;
+                    }
+                    nbstart = __ldg(tab + (c + 1) * kTabInts + 17);
+                    nbcount = __ldg(tab + (c + 1) * kTabInts + 18);
+                }
                 if (k >= kStages)
                     ok = mbar_wait(smem_u32(&bar_empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_abort);
                 if (!ok) break;
                 const unsigned full = smem_u32(&bar_full[s]);
                 const unsigned dst = smem_u32(stage_mem) + (unsigned)(s * L::kBytes);
-                if (r == 0) {
+                if (r0 == 0) {
                     mbar_expect(full, (unsigned)(rows * kRowBytes + bcount * 18 + kTabInts * 4));
                     bulk_g2s(dst + L::kTab, tab + c * kTabInts, kTabInts * 4, full);
                     if (bcount > 0) {
@@ -526,8 +546,13 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
                         bulk_g2s(dst + L::kRow, tl.erow + gb + bstart, (unsigned)(bcount * 2), full);
                     }
                 }
-                if (r < rows)
-                    bulk_g2s(dst + (unsigned)(r * kRowBytes), slab + (size_t)cell * kRowFloats, kRowBytes, full);
+#pragma unroll
+                for (int i = 0; i < kRowsPerThread; ++i) {
+                    const int r = r0 + kProducers * i;
+                    if (r < rows)
+                        bulk_g2s(dst + (unsigned)(r * kRowBytes), slab + (size_t)cell[i] * kRowFloats, kRowBytes,
+                                 full);
+                }
             }
         }
         if (!ok) {
