@@ -4,30 +4,35 @@
 // R[v, h] = sum_g w(v, g) I[g, h] needs one slab row I[g, block] per
 // (voxel, nonzero neighbor).  Voxels that are close in the visiting order see
 // mostly the same cells: on the 256 x 256 city the union of the lists of 64
-// consecutive voxels is 7.6x smaller than their sum (10.6x for 128).  So:
+// consecutive voxels is 7.6x smaller than their sum, and 4 consecutive voxels
+// share 1.9x.  So, once per run (hour-independent):
 //
-//   build (once per run, hour-independent): voxels are cut into aligned
-//     groups of at most G positions of the visiting order (halved until the
-//     group's nonzero entries fit kTileCap); per group, the union of its
-//     cells (sorted descending, as the ba-RLE lists are) replaces the cells
-//     in the weighted-list buffer, and each entry becomes (slot, w) with
-//     slot = the cell's index in the union, entries of a voxel in ascending
-//     slot order;
-//   per hour block: a CTA takes a group; a producer warp streams the union
-//     rows I[g, block] into a ring of shared-memory stages with
-//     cp.async.bulk (one bulk copy per 1 KB row, completion counted on an
-//     mbarrier); 16 consumer warps each own 4 voxels (G = 64: with 17
-//     warps a sub-partition holds 5, which caps registers at 96 a thread,
-//     room for 4 voxels x 8 hours of accumulators), keep their entry
-//     windows in registers and apply the entries whose slot falls in the
-//     current stage (lanes hold hours, FMA per hour as in k_reflect_group),
-//     then add each voxel's own direct + diffuse and accumulate.
+//   groups   aligned runs of at most 64 positions of the visiting order,
+//            halved until the group's nonzero entries fit kTileCap;
+//   union    the group's distinct cells, sorted descending (the ba-RLE list
+//            order), replace the cells in the weighted-list buffer; each
+//            entry becomes (slot = index in the union, w), ascending per voxel;
+//   quads    the slot lists of each 4 consecutive voxels are merged: one
+//            entry per distinct slot with the 4 weights (0 where a voxel
+//            lacks the slot);
+//   chunks   the union is cut into chunks of R rows (what one shared-memory
+//            stage holds); the merged entries are laid out chunk by chunk,
+//            quads in order inside a chunk, with a table of quad offsets.
 //
-// Per voxel, entries are applied in ascending slot order = descending cell
-// order, which is the ba-RLE list order, so on ba-RLE lists the result is
-// bit-identical to the per-voxel kernel (group size 1).  Every wait on an
-// mbarrier is bounded (kWaitNs): on expiry the kernel sets kErrWaitTimeout,
-// stops, lets its own bulk copies land (bounded as well) and returns.
+// Per hour block, a CTA per group in turn (persistent grid): 4 producer warps
+// copy each chunk's R union rows I[g, block] (one cp.async.bulk per 1 KB
+// row, one row per thread) plus its entry block and table into a stage;
+// completion is counted in bytes on the stage's mbarrier.  16 consumer warps
+// each own a quad: for every entry of the chunk, one shared-memory row read
+// feeds 4 x Q FMAs per lane (lanes hold hours).  After the last chunk each
+// voxel adds its own direct + diffuse (its own slab row) and accumulates.
+//
+// Per voxel the FMAs run in ascending slot order = descending cell order,
+// with exact zero terms where the quad's other voxels have a slot, so on
+// ba-RLE lists the result is bit-identical to the per-voxel kernel (group
+// size 1).  Every wait on an mbarrier is bounded (kWaitNs): on expiry the
+// kernel sets kErrWaitTimeout, stops, lets its bulk copies land (bounded as
+// well) and returns.
 #include "solar_math.cuh"
 
 namespace sgb {
