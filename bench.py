@@ -42,10 +42,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="dsm1024")
-    ap.add_argument("--format", type=int, default=1, help="0 = CSR, 1 = ba-RLE")
+    ap.add_argument("--format", type=int, default=0, help="0 = CSR, 1 = ba-RLE")
     ap.add_argument("--hour-block", type=int, default=256)
     ap.add_argument("--accumulation", type=int, default=1)
-    ap.add_argument("--group-size", type=int, default=1)
+    ap.add_argument("--group-size", type=int, default=64)
     ap.add_argument("--ref-workload", default="dsm256",
                     help="reference arm: workload timed per step (a full reference run of dsm1024 takes ~6 min)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-hour comparison run")
@@ -167,8 +167,10 @@ def roofline_bytes(scene, ctx_sizes, fmt, B, acc, V, entries, staged_rows=0) -> 
              voxel; slab rows of the top cells.
       V = 1, 2, 4, 8: entries of one cell id + V weights, group offsets; the
              slab has a row for every voxel (its own term).
-      V = 64 (tiles): entries of a 2-byte slot + weight, the groups' union
-             cell ids, offsets; slab rows of every voxel."""
+      V = 64 (tiles): merged entries of a 2-byte row index + the 4 weights of
+             a voxel quad, the groups' union cell ids and chunk tables (80 B
+             per chunk of 80 rows, ~1 B per staged row), offsets; slab rows of
+             every voxel."""
     csr_entries, barle_bytes, words32 = ctx_sizes
     N, T = scene.num_total, scene.num_top
     acc_b = 16 if acc in (0, 1) else 8
@@ -176,7 +178,7 @@ def roofline_bytes(scene, ctx_sizes, fmt, B, acc, V, entries, staged_rows=0) -> 
         lists = (barle_bytes if fmt == 1 else 4 * csr_entries) + 8 * (N + 1)
         return float(lists + N * (4 + 32 + 4 * words32 + acc_b) + T * B * 4)
     if V >= 64:
-        lists = entries * 6 + staged_rows * 4 + 8 * (N + 1)
+        lists = entries * 18 + staged_rows * 5 + 8 * (N + 1)
     else:
         lists = entries * (4 + 4 * V) + 8 * (N // V + 2)
     return float(lists + N * (4 + acc_b) + N * B * 4)
@@ -279,8 +281,8 @@ def run_ours(args, world, rank, local, pg):
                 except ValueError:
                     pass
     if V >= 64:
-        kdesc = (f"k_reflect_tile<{B // 32},{V // 16}> (hour-block sparse x dense product, union rows of {V}-voxel "
-                 f"groups staged in shared memory by cp.async.bulk + accumulation)")
+        kdesc = (f"k_reflect_tile<{B // 32}> (hour-block sparse x dense product: union rows of {V}-voxel groups "
+                 f"staged in shared memory by cp.async.bulk, merged 4-voxel entries, + accumulation)")
     elif V >= 1:
         kdesc = f"k_reflect_group<{B // 32},{V}> (hour-block sparse x dense product over weighted lists + accumulation)"
     else:
@@ -294,7 +296,20 @@ def run_ours(args, world, rank, local, pg):
             "gathered_slab_bytes_per_launch": gathered,
             "gather_gbs": round(gathered / (per_launch_ms / 1e3) / 1e9, 1) if per_launch_ms > 0 else None}
     if V >= 64:
+        # the tile kernel's binding resource: shared-memory reads (one row of
+        # B floats + the 18-byte entry per merged entry) against the SM data
+        # path, 128 B per clock per SM at the median SM clock of the run
         roof["staged_slab_bytes_per_launch"] = float(staged) * B * 4
+        smem_bytes = float(entries) * (B * 4 + 18)
+        sm_mhz = clocks.get("sm_mhz") or 0.0
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        smem_peak = sms * 128 * sm_mhz * 1e6 / 1e9
+        roof["smem"] = {"bytes_per_launch": smem_bytes,
+                        "achieved_gbs": round(smem_bytes / (per_launch_ms / 1e3) / 1e9, 1) if per_launch_ms > 0 else None,
+                        "peak_gbs": round(smem_peak, 1) if smem_peak else None,
+                        "frac": round(smem_bytes / (per_launch_ms / 1e3) / 1e9 / smem_peak, 4)
+                        if smem_peak and per_launch_ms > 0 else None,
+                        "peak_note": "148 SMs x 128 B/clk x median SM clock under load"}
 
     # ---- end to end through the host API (pinned host buffers in and out)
     e2e = None
