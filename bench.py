@@ -295,6 +295,20 @@ def run_ours(args, world, rank, local, pg):
             "dominant_group": dom[0],
             "gathered_slab_bytes_per_launch": gathered,
             "gather_gbs": round(gathered / (per_launch_ms / 1e3) / 1e9, 1) if per_launch_ms > 0 else None}
+    if V >= 1:
+        # the product's arithmetic: one FMA per nonzero weight and hour, against
+        # the FP32 pipe (148 SMs x 128 FMA/clk x 2 flops at the median SM clock)
+        wents = ctx.weighted_entries()
+        sm_mhz = clocks.get("sm_mhz") or 0.0
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+        flops = 2.0 * wents * B
+        roof["fp32"] = {"useful_flop_per_launch": flops,
+                        "achieved_tflops": round(flops / (per_launch_ms / 1e3) / 1e12, 2) if per_launch_ms > 0 else None,
+                        "peak_tflops": round(fp32_peak, 1) if fp32_peak else None,
+                        "frac": round(flops / (per_launch_ms / 1e3) / 1e12 / fp32_peak, 4)
+                        if fp32_peak and per_launch_ms > 0 else None,
+                        "peak_note": "FP32 FMA pipe: SMs x 128 lanes x 2 flop x median SM clock under load"}
     if V >= 64:
         # the tile kernel's binding resource: shared-memory reads (one row of
         # B floats + the 18-byte entry per merged entry) against the SM data

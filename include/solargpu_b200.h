@@ -186,6 +186,10 @@ long long solar_gpu_last_reflection_entries(solar_gpu_context* ctx);
    other kernels. */
 long long solar_gpu_last_staged_rows(solar_gpu_context* ctx);
 
+/* Nonzero reflection weights (receiver, neighbor pairs) of the last run with
+   group_size >= 1: each contributes one FMA per daylight hour; 0 otherwise. */
+long long solar_gpu_last_weighted_entries(solar_gpu_context* ctx);
+
 /* Number of kernel launches the library issued in the last run. */
 long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
 

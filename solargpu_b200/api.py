@@ -70,6 +70,8 @@ def lib() -> C.CDLL:
         L.solar_gpu_last_reflection_entries.argtypes = [vp]
         L.solar_gpu_last_staged_rows.restype = ll
         L.solar_gpu_last_staged_rows.argtypes = [vp]
+        L.solar_gpu_last_weighted_entries.restype = ll
+        L.solar_gpu_last_weighted_entries.argtypes = [vp]
         for name in ("solar_gpu_uncompressed_gpu_irradiance", "solar_gpu_compressed_gpu_irradiance"):
             fn = getattr(L, name)
             fn.argtypes = [vp, i, i, i, i, vp, vp, f, vp, i, vp, i, vp, i, vp, vp, vp]
@@ -288,6 +290,10 @@ class Context:
     def staged_rows(self) -> int:
         """Slab rows the tile kernel staged per hour block in the last run."""
         return int(lib().solar_gpu_last_staged_rows(self.h))
+
+    def weighted_entries(self) -> int:
+        """Nonzero reflection weights of the last run (one FMA per hour each)."""
+        return int(lib().solar_gpu_last_weighted_entries(self.h))
 
     def launches(self) -> int:
         return int(lib().solar_gpu_last_launch_count(self.h))

@@ -94,6 +94,7 @@ struct solar_gpu_context {
     long long launches = 0;
     long long group_entries = 0;
     long long staged_rows = 0;   // slab rows the tile kernel stages per hour block
+    long long weighted_entries = 0;   // nonzero reflection weights of the last run
     bool timed = false;
     // per kernel-group event log (time_kernels)
     bool ktime = false;
@@ -499,6 +500,7 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
             }
             long long Ew = 0;
             RK(read_ll(c, as<long long>(c->w_off) + N, &Ew, st));
+            c->weighted_entries = Ew;
             RK(ensure(c->w_cell, sizeof(int) * (size_t)(Ew + 1)));
             RK(ensure(c->w_val, sizeof(float) * (size_t)(Ew + 1)));
             {
@@ -675,6 +677,7 @@ int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const sola
     c->ktime = o->time_kernels != 0;
     c->group_entries = 0;
     c->staged_rows = 0;
+    c->weighted_entries = 0;
     c->kt_used = 0;
     c->kt_ids.clear();
     c->kt_stream = st;
@@ -915,6 +918,8 @@ long long solar_gpu_last_launch_count(solar_gpu_context* c) { return c ? c->laun
 long long solar_gpu_last_reflection_entries(solar_gpu_context* c) { return c ? c->group_entries : -1; }
 
 long long solar_gpu_last_staged_rows(solar_gpu_context* c) { return c ? c->staged_rows : -1; }
+
+long long solar_gpu_last_weighted_entries(solar_gpu_context* c) { return c ? c->weighted_entries : -1; }
 
 int solar_gpu_kernel_times(solar_gpu_context* c, double* ms, long long* launches, int n)
 {
