@@ -84,7 +84,7 @@ struct solar_gpu_context {
         in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
-        tile_erow, tile_ew;
+        tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
@@ -329,20 +329,36 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         RK(ensure(c->barle_bytes, (size_t)N * 160));
     }
     const DevScene ds = dev_scene(s);
-    // One chunk: rows follow the visiting order (Morton-adjacent voxels share
-    // a warp, so their rays have similar lengths).  Several chunks: index order.
+    // Rows follow the visiting order (Morton-adjacent voxels share a warp, so
+    // their rays have similar lengths); with several chunks, each chunk (a
+    // range of voxel indices) is traced in the visiting order of its voxels.
     const int* perm = nullptr;
     const int* inv = nullptr;
+    RK(ensure(c->order_inv, sizeof(int) * (size_t)N));
     if (chunk >= N) {
-        RK(ensure(c->order_inv, sizeof(int) * (size_t)N));
         CK(launch_invert(as<int>(c->order), N, as<int>(c->order_inv), st));
         perm = as<int>(c->order);
         inv = as<int>(c->order_inv);
         c->launches += 1;
+    } else {
+        RK(ensure(c->chunk_perm, sizeof(int) * (size_t)chunk));
+        RK(ensure(c->chunk_flag, sizeof(int) * (size_t)N));
+        RK(ensure(c->chunk_pos, sizeof(long long) * ((size_t)N + 1)));
+        RK(ensure(c->chunk_tmp, sizeof(long long) * scan_scratch_elems(N)));
+        perm = as<int>(c->chunk_perm);
+        inv = as<int>(c->order_inv);
     }
     long long csr_total = 0, barle_total = 0;
     for (long long v0 = 0; v0 < N; v0 += chunk) {
         const int n = (int)((N - v0) < chunk ? (N - v0) : chunk);
+        if (chunk < N) {
+            KScope k(c, SOLAR_GPU_KT_SETUP);
+            CK(launch_chunk_order(as<int>(c->order), N, (int)v0, n, as<int>(c->chunk_flag),
+                                  as<long long>(c->chunk_pos), as<long long>(c->chunk_tmp),
+                                  as<int>(c->chunk_perm), st));
+            CK(launch_invert(as<int>(c->chunk_perm), n, as<int>(c->order_inv), st));
+            c->launches += 6;
+        }
         {
             KScope k(c, SOLAR_GPU_KT_TRACE);
             CK(launch_trace(ds, as<DirEntry>(c->dirs), D, c->words32, (int)v0, n, as<int>(c->raw),
@@ -768,7 +784,7 @@ int solar_gpu_create(int device, solar_gpu_context** out)
     return SOLAR_GPU_OK;
 }
 
-static constexpr int kNumBufs = 61;
+static constexpr int kNumBufs = 65;
 
 static void all_bufs(solar_gpu_context* c, DevBuf** out)
 {
@@ -782,7 +798,8 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                       &c->w_cell, &c->w_val, &c->order_first, &c->order_inv,
                                 &c->tile_flag, &c->tile_pos, &c->tile_start, &c->tile_union, &c->tile_slot,
                                 &c->tile_rows, &c->tile_gcnt, &c->tile_gnch, &c->tile_gbase, &c->tile_tbase,
-                                &c->tile_table, &c->tile_erow, &c->tile_ew};
+                                &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
+                                &c->chunk_pos, &c->chunk_tmp};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

@@ -66,15 +66,20 @@ void set_last_error(const char* msg);
 // ------------------------------------------------------------------ launchers
 
 // tracer (trace.cu)
-// Stage 1 kernels address rows of the raw hit buffer.  Row lv holds voxel
-// perm[lv] when a permutation is given (counts, sizes indexed by voxel),
-// else voxel voxel_offset + lv; kernels that iterate voxels take the inverse.
+// Stage 1 kernels address rows of the raw hit buffer of a chunk of voxels
+// [voxel_offset, voxel_offset + chunk_count).  Row lv holds chunk voxel
+// perm[lv] when a permutation is given (counts, sizes indexed by chunk
+// voxel), else chunk voxel lv; kernels that iterate voxels take the inverse.
 cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
                          int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
                          const int* perm, cudaStream_t st);
 cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, const int* perm,
                           cudaStream_t st);
 cudaError_t launch_invert(const int* perm, int n, int* inv, cudaStream_t st);
+// perm = the chunk voxels [v0, v0 + n) (as v - v0) in visiting order;
+// flag [N] and pos [N + 1] scratch.
+cudaError_t launch_chunk_order(const int* order, int N, int v0, int n, int* flag, long long* pos,
+                               long long* scan_tmp, int* perm, cudaStream_t st);
 cudaError_t launch_scan_counts(const int* counts, int n, long long base, long long* offsets,
                                long long* block_sums, int* block_tmp, cudaStream_t st);
 size_t scan_scratch_elems(int n);

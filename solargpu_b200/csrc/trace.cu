@@ -66,9 +66,9 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
     __shared__ int stage[kRawGroup][kTraceBlock];
     const int lv = blockIdx.x * kTraceBlock + threadIdx.x;
     const bool active = lv < chunk_count;
-    // Row lv traces voxel perm[lv] (visiting order: Morton-adjacent lanes walk
-    // similar rays) or voxel_offset + lv.
-    const int v = perm ? __ldg(perm + (active ? lv : 0)) : voxel_offset + (active ? lv : 0);
+    // Row lv traces voxel voxel_offset + perm[lv] (visiting order: Morton-
+    // adjacent lanes walk similar rays) or voxel_offset + lv.
+    const int v = voxel_offset + (perm ? __ldg(perm + (active ? lv : 0)) : (active ? lv : 0));
     const int top = __ldg(s.pix_parent + v);
     const int gx = top % s.W;
     const int gy = top / s.W;
@@ -310,6 +310,33 @@ __global__ void k_invert(const int* __restrict__ perm, int n, int* __restrict__ 
     if (i < n) inv[perm[i]] = i;
 }
 }  // namespace
+
+namespace {
+__global__ void k_chunk_flags(const int* __restrict__ order, int N, int v0, int n, int* __restrict__ flag)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < N) flag[p] = (unsigned)(order[p] - v0) < (unsigned)n ? 1 : 0;
+}
+
+__global__ void k_chunk_scatter(const int* __restrict__ order, int N, int v0, const int* __restrict__ flag,
+                                const long long* __restrict__ pos, int* __restrict__ perm)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < N && flag[p]) perm[pos[p]] = order[p] - v0;
+}
+}  // namespace
+
+cudaError_t launch_chunk_order(const int* order, int N, int v0, int n, int* flag, long long* pos,
+                               long long* scan_tmp, int* perm, cudaStream_t st)
+{
+    if (N <= 0 || n <= 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((N + 255) / 256);
+    k_chunk_flags<<<grid, 256, 0, st>>>(order, N, v0, n, flag);
+    cudaError_t e = launch_scan_counts(flag, N, 0, pos, scan_tmp, nullptr, st);
+    if (e != cudaSuccess) return e;
+    k_chunk_scatter<<<grid, 256, 0, st>>>(order, N, v0, flag, pos, perm);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_invert(const int* perm, int n, int* inv, cudaStream_t st)
 {

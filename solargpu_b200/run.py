@@ -1,13 +1,17 @@
 """Command-line runner: the annual irradiance path on a named synthetic workload.
 
-    python -m solargpu_b200.run --workload dsm1024 [--format 1] [--hour-block 256]
-                                [--group-size 1] [--accumulation 1] [--runs 2] [--out file.npy]
+    python -m solargpu_b200.run --workload dsm1024 [--format 0] [--hour-block 256]
+                                [--group-size 64] [--accumulation 1] [--runs 2] [--out file.npy]
+                                [--compare-accumulation]
 
 Plays the role of the reference CLI (src/main.cpp) for generated scenes:
 builds the seeded DSM, voxelizes it, computes the sun series and TMY, runs
 the CUDA pipeline `--runs` times on device-resident inputs and prints the
 stage and kernel-group times of the last run.  Also the profiling driver
-(run it under ncu with -k/-s/-c filters).
+(run it under ncu with -k/-s/-c filters).  --compare-accumulation runs the
+three accumulation modes (FP64 block sums, Kahan FP32, plain FP32) on the
+same scene and reports the relative differences of the last two from the
+first, with each mode's time.
 """
 from __future__ import annotations
 
@@ -21,13 +25,14 @@ import numpy as np
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--workload", default="dsm1024")
-    ap.add_argument("--format", type=int, default=1, help="0 = CSR, 1 = ba-RLE")
+    ap.add_argument("--format", type=int, default=0, help="0 = CSR, 1 = ba-RLE")
     ap.add_argument("--hour-block", type=int, default=256)
-    ap.add_argument("--group-size", type=int, default=1)
+    ap.add_argument("--group-size", type=int, default=64)
     ap.add_argument("--accumulation", type=int, default=1)
     ap.add_argument("--chunk-voxels", type=int, default=0)
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--out", default=None, help="write the annual irradiance (float32 .npy)")
+    ap.add_argument("--compare-accumulation", action="store_true")
     a = ap.parse_args(argv)
 
     import torch
@@ -39,6 +44,26 @@ def main(argv=None) -> int:
          "wall_z": torch.from_numpy(s.wall_z if s.wall_z.size else np.zeros(1, np.float32)).to(dev),
          "slopes": torch.from_numpy(s.slopes).to(dev), "aspects": torch.from_numpy(s.aspects).to(dev)}
     out = torch.zeros(s.num_total, dtype=torch.float32, device=dev)
+    if a.compare_accumulation:
+        res, ms = {}, {}
+        with api.Context(0) as ctx:
+            for acc in (0, 1, 2):
+                ctx.run_device(s, d, out, neighbor_format=a.format, hour_block=a.hour_block,
+                               group_size=a.group_size, accumulation=acc, chunk_voxels=a.chunk_voxels,
+                               use_graph=1, time_kernels=0)
+                torch.cuda.synchronize()
+                ms[acc] = round(ctx.timings()[3], 1)
+                res[acc] = out.double().clone()
+        ref = res[0]
+        den = ref.abs().clamp_min(1.0)
+        cmp = {}
+        for acc, name in ((1, "kahan_fp32"), (2, "plain_fp32")):
+            r = (res[acc] - ref).abs() / den
+            cmp[name] = {"max_rel_vs_fp64_sums": float(r.max()), "mean_rel_vs_fp64_sums": float(r.mean())}
+        print(json.dumps({"workload": a.workload, "voxels": s.num_total, "top_voxels": s.num_top,
+                          "total_ms": {"fp64_sums": ms[0], "kahan_fp32": ms[1], "plain_fp32": ms[2]},
+                          "accumulation": cmp}))
+        return 0
     with api.Context(0) as ctx:
         for _ in range(max(1, a.runs)):
             ctx.run_device(s, d, out, neighbor_format=a.format, hour_block=a.hour_block,
