@@ -495,8 +495,6 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         // Rows for the top cells (neighbor values); the weighted-list kernels
         // also read each voxel's own row, so there the slab covers all voxels.
         const int slab_rows = o->group_size > 0 ? N : T;
-        RK(ensure(c->slab, sizeof(float) * (size_t)slab_rows * B));
-        float* slab = as<float>(c->slab);
         GroupLists gl{o->group_size, nullptr, nullptr, nullptr};
         TileLists tl{};
         const bool tiled = o->group_size >= 64;
@@ -552,9 +550,8 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(launch_tile_build((int)NG, as<int>(c->tile_start), as<long long>(c->w_off),
-                                         as<int>(c->w_cell), as<float>(c->w_val),
-                                         as<unsigned short>(c->tile_slot), as<int>(c->tile_union),
-                                         as<long long>(c->tile_rows), err, st));
+                                         as<int>(c->w_cell), as<unsigned short>(c->tile_slot),
+                                         as<int>(c->tile_union), as<long long>(c->tile_rows), err, st));
                 }
                 RK(read_ll(c, as<long long>(c->tile_rows), &c->staged_rows, st));
                 const int R = tile_rows_per_stage(B);
@@ -590,6 +587,17 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 }
                 c->launches += 10;
                 c->group_entries = Em;
+                // Per-voxel weights and slots are dead now; above 1/16 of the
+                // device (scenes of tens of millions of voxels) they are
+                // released to make room for the slab.
+                size_t fr = 0, tot = 0;
+                CK(cudaMemGetInfo(&fr, &tot));
+                if (c->w_val.cap + c->tile_slot.cap > tot / 16) {
+                    CK(cudaFree(c->w_val.p));
+                    CK(cudaFree(c->tile_slot.p));
+                    c->w_val.p = c->tile_slot.p = nullptr;
+                    c->w_val.cap = c->tile_slot.cap = 0;
+                }
                 tl.G = V;
                 tl.NG = (int)NG;
                 tl.start = as<int>(c->tile_start);
@@ -631,6 +639,10 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 gl.weights = as<float>(c->grp_w);
             }
         }
+        // allocated after the once-per-run builds, whose intermediates may
+        // have been released to make room (very large scenes)
+        RK(ensure(c->slab, sizeof(float) * (size_t)slab_rows * B));
+        float* slab = as<float>(c->slab);
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         const bool use_graph = o->use_graph != 0 && !c->ktime;

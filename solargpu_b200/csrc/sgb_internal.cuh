@@ -182,10 +182,11 @@ cudaError_t launch_tile_groups(int N, int G, const long long* woff, int* flag, l
                                long long* scan_tmp, int* start, cudaStream_t st);
 // Union rows per chunk of the tile kernel for hour block B (0 if not built).
 int tile_rows_per_stage(int B);
-// Rewrites the weighted lists of each group in place into union + slots;
-// rows_total = sum of the unions (slab rows staged per hour block).
-cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, float* wts,
-                              unsigned short* slots, int* unions, long long* rows_total, int* err, cudaStream_t st);
+// Per group: the union of its cells (descending) written over the start of
+// the group's cells, and each entry's slot in it; rows_total = sum of the
+// unions (slab rows staged per hour block).
+cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, unsigned short* slots,
+                              int* unions, long long* rows_total, int* err, cudaStream_t st);
 // Merges the slot lists of each quad and lays them out chunk by chunk:
 // pass 0 counts (gcnt: padded merged entries, gnch: chunks, per group),
 // pass 1 writes at gbase / tbase (scans of gcnt / gnch); ew must be zero.

@@ -11,7 +11,7 @@
 //            halved until the group's nonzero entries fit kTileCap;
 //   union    the group's distinct cells, sorted descending (the ba-RLE list
 //            order), replace the cells in the weighted-list buffer; each
-//            entry becomes (slot = index in the union, w), ascending per voxel;
+//            entry gets its slot (index in the union);
 //   quads    the slot lists of each 4 consecutive voxels are merged: one
 //            entry per distinct slot with the 4 weights (0 where a voxel
 //            lacks the slot);
@@ -78,7 +78,7 @@ __global__ void k_tile_starts(int N, const int* __restrict__ flag, const long lo
 
 // ---- build -------------------------------------------------------------------
 
-__device__ __forceinline__ void block_bitonic(uint32_t* keys, float* vals, int n2, bool descending)
+__device__ __forceinline__ void block_bitonic(uint32_t* keys, int n2, bool descending)
 {
     for (int size = 2; size <= n2; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
@@ -90,11 +90,6 @@ __device__ __forceinline__ void block_bitonic(uint32_t* keys, float* vals, int n
                 if ((a > b) == up) {
                     keys[i] = b;
                     keys[j] = a;
-                    if (vals) {
-                        const float x = vals[i];
-                        vals[i] = vals[j];
-                        vals[j] = x;
-                    }
                 }
             }
             __syncthreads();
@@ -103,20 +98,16 @@ __device__ __forceinline__ void block_bitonic(uint32_t* keys, float* vals, int n
 }
 
 // One CTA per group.  Shared memory: a hash set of the group's cells
-// (2 x kTileCap slots, load <= 1/2), reused afterwards for the (voxel, slot)
-// keys and weights; the union (kTileCap).
+// (2 x kTileCap slots, load <= 1/2) and the union (kTileCap).
 __global__ void __launch_bounds__(kBuildThreads)
 k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, int* __restrict__ cells,
-             float* __restrict__ wts, unsigned short* __restrict__ slots, int* __restrict__ unions,
+             unsigned short* __restrict__ slots, int* __restrict__ unions,
              unsigned long long* __restrict__ rows_total, int* __restrict__ err)
 {
     constexpr int kHashSlots = 2 * kTileCap;
     extern __shared__ __align__(16) uint32_t sm[];
     uint32_t* table = sm;                                     // [kHashSlots], key = cell + 1, 0 = empty
-    uint32_t* keys = sm;                                      // [kTileCap] after the union is built
-    float* vals = reinterpret_cast<float*>(sm + kTileCap);    // [kTileCap]
     uint32_t* uni = sm + kHashSlots;                          // [kTileCap]
-    __shared__ int s_off[257];
     __shared__ int s_count;
     const int q = blockIdx.x;
     const int p0 = start[q], p1 = start[q + 1];
@@ -131,7 +122,6 @@ k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, 
         return;
     }
     const int n = (int)nl;
-    for (int j = threadIdx.x; j <= nv; j += blockDim.x) s_off[j] = (int)(woff[p0 + j] - e0);
     for (int i = threadIdx.x; i < kHashSlots; i += blockDim.x) table[i] = 0u;
     if (threadIdx.x == 0) s_count = 0;
     __syncthreads();
@@ -156,45 +146,24 @@ k_tile_build(const int* __restrict__ start, const long long* __restrict__ woff, 
     while (u2 < u) u2 <<= 1;
     for (int i = u + threadIdx.x; i < u2; i += blockDim.x) uni[i] = 0u;
     __syncthreads();
-    block_bitonic(uni, nullptr, u2, true);   // descending cell order
+    block_bitonic(uni, u2, true);   // descending cell order
     int* ucell = reinterpret_cast<int*>(uni);
     for (int i = threadIdx.x; i < u; i += blockDim.x) ucell[i] = (int)uni[i] - 1;
     __syncthreads();
 
-    // entries -> (local voxel << 16 | slot), weights alongside
-    int n2 = kBuildThreads;
-    while (n2 < n) n2 <<= 1;
-    bool unsorted = false;
-    for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-        uint32_t k = 0xFFFFFFFFu;
-        float w = 0.0f;
-        if (i < n) {
-            const int cell = cells[e0 + i];
-            int lo = 0, hi = u - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (ucell[mid] > cell) lo = mid + 1; else hi = mid;
-            }
-            int a = 0, b = nv;   // largest j with s_off[j] <= i
-            while (b - a > 1) {
-                const int mid = (a + b) >> 1;
-                if (s_off[mid] <= i) a = mid; else b = mid;
-            }
-            k = ((uint32_t)a << 16) | (uint32_t)lo;
-            w = wts[e0 + i];
+    // each entry's slot (its cell's index in the union); entry order and
+    // weights are unchanged (the quad merge sorts by slot)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int cell = cells[e0 + i];
+        int lo = 0, hi = u - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (ucell[mid] > cell) lo = mid + 1; else hi = mid;
         }
-        keys[i] = k;
-        vals[i] = w;
+        slots[e0 + i] = (unsigned short)lo;
     }
     __syncthreads();
-    for (int i = threadIdx.x + 1; i < n; i += blockDim.x) unsorted |= keys[i] < keys[i - 1];
-    if (__syncthreads_or(unsorted)) block_bitonic(keys, vals, n2, false);
-
     for (int i = threadIdx.x; i < u; i += blockDim.x) cells[e0 + i] = ucell[i];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        slots[e0 + i] = (unsigned short)(keys[i] & 0xFFFFu);
-        wts[e0 + i] = vals[i];
-    }
     if (threadIdx.x == 0) {
         unions[q] = u;
         atomicAdd(rows_total, (unsigned long long)u);
@@ -700,8 +669,8 @@ cudaError_t launch_tile_groups(int N, int G, const long long* woff, int* flag, l
     return cudaGetLastError();
 }
 
-cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, float* wts,
-                              unsigned short* slots, int* unions, long long* rows_total, int* err, cudaStream_t st)
+cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, int* cells, unsigned short* slots,
+                              int* unions, long long* rows_total, int* err, cudaStream_t st)
 {
     if (NG <= 0) return cudaSuccess;
     const size_t smem = (size_t)3 * kTileCap * 4;
@@ -710,7 +679,7 @@ cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, i
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(rows_total, 0, sizeof(long long), st);
     if (e != cudaSuccess) return e;
-    k_tile_build<<<NG, kBuildThreads, smem, st>>>(start, woff, cells, wts, slots, unions,
+    k_tile_build<<<NG, kBuildThreads, smem, st>>>(start, woff, cells, slots, unions,
                                                   reinterpret_cast<unsigned long long*>(rows_total), err);
     return cudaGetLastError();
 }
