@@ -24,6 +24,7 @@ namespace sgb {
 namespace {
 
 constexpr int kTraceBlock = 128;
+constexpr int kDirParts = 8;       // blocks per voxel block, each an eighth of the directions
 constexpr int kDedupeWarps = 4;
 constexpr int kHashSlots = 4096;   // > 2592 possible distinct hits per voxel
 constexpr int kDedupeBatch = 9;    // 2592 = 9 batches of 9 rounds of 32 directions
@@ -74,10 +75,14 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
     const int gy = top / s.W;
     const float base_z = (v < s.T) ? __ldg(s.grid + top) : __ldg(s.wall_z + (v - s.T));
 
+    // this block's directions: groups [gb, ge) of kRawGroup
+    const int ngroups = (D + kRawGroup - 1) / kRawGroup;
+    const int gb = (int)((long long)ngroups * blockIdx.y / gridDim.y);
+    const int ge = (int)((long long)ngroups * (blockIdx.y + 1) / gridDim.y);
     uint32_t acc = 0;
     int cur_word = -1;
     int* row = raw + (size_t)(active ? lv : 0) * D;
-    for (int g0 = 0; g0 < D; g0 += kRawGroup) {
+    for (int g0 = gb * kRawGroup; g0 < ge * kRawGroup; g0 += kRawGroup) {
         for (int k = 0; k < kRawGroup; ++k) {
             const DirEntry d = dirs[g0 + k];
             const int hit = active ? trace_ray(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d) : 0;
@@ -86,7 +91,8 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
             if (dense >= 0) {
                 const int w = dense >> 5;
                 if (w != cur_word) {
-                    if (active && acc) shadow[(size_t)v * words32 + cur_word] = acc;
+                    // a word may be shared with the neighbouring direction part
+                    if (active && acc) atomicOr(shadow + (size_t)v * words32 + cur_word, acc);
                     acc = 0;
                     cur_word = w;
                 }
@@ -101,7 +107,7 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
                                    stage[4 * q + 2][threadIdx.x], stage[4 * q + 3][threadIdx.x]);
         }
     }
-    if (active && acc && cur_word >= 0) shadow[(size_t)v * words32 + cur_word] = acc;
+    if (active && acc && cur_word >= 0) atomicOr(shadow + (size_t)v * words32 + cur_word, acc);
 }
 
 __device__ __forceinline__ uint32_t hash_slot(uint32_t x)
@@ -262,7 +268,9 @@ cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int wor
                          const int* perm, cudaStream_t st)
 {
     if (chunk_count <= 0) return cudaSuccess;
-    const int grid = (chunk_count + kTraceBlock - 1) / kTraceBlock;
+    // D is a multiple of kRawGroup (rows are written kRawGroup directions at a time)
+    if (D % kRawGroup != 0) return cudaErrorInvalidValue;
+    const dim3 grid((chunk_count + kTraceBlock - 1) / kTraceBlock, kDirParts);
     k_trace<<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow, perm);
     return cudaGetLastError();
 }
