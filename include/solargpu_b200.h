@@ -65,6 +65,9 @@ typedef struct solar_gpu_options {
                                 per group (B 64..256) */
 } solar_gpu_options;
 
+/* CSR lists, hour block 256, FP64 block sums, hourly reflection, chunk from
+   free memory, CUDA graph on, no kernel timing, group size 64 (the tile
+   kernel).  The drop-in entry points run with these, format aside. */
 void solar_gpu_default_options(solar_gpu_options* opt);
 
 /* ---- drop-in entry points (synchronous, host buffers, device 0) -------- */

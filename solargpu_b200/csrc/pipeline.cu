@@ -766,13 +766,13 @@ void solar_gpu_default_options(solar_gpu_options* o)
 {
     if (!o) return;
     o->neighbor_format = SOLAR_GPU_CSR;
-    o->hour_block = 128;
+    o->hour_block = 256;
     o->accumulation = SOLAR_GPU_ACC_FP64;
     o->reflection = SOLAR_GPU_REFL_HOURLY;
     o->chunk_voxels = 0;
     o->use_graph = 1;
     o->time_kernels = 0;
-    o->group_size = 8;
+    o->group_size = 64;
 }
 
 const char* solar_gpu_last_error(void) { return g_err.c_str(); }
