@@ -155,6 +155,32 @@ int solar_gpu_trace_sizes(solar_gpu_context* ctx, long long* csr_entries, long l
    barle_bytes [barle_bytes] (byte-identical to the reference encoder),
    shadow [N][shadow_words] uint32 (bit b of word w set = dense sun bin 32w+b
    is blocked for that voxel). */
+/* Stage 1 products handed back to the library (host arrays), e.g. read from
+   an on-disk cache: one list format plus the shadow words, laid out as
+   solar_gpu_trace_copy returns them. */
+typedef struct solar_gpu_lists {
+    int format;                  /* SOLAR_GPU_CSR or SOLAR_GPU_BARLE */
+    const long long* offsets;    /* [N + 1], offsets[0] = 0, offsets[N] = data_size */
+    const void* data;            /* CSR ids (int32, 1-based cells) or ba-RLE bytes */
+    long long data_size;         /* ids (CSR) or bytes (ba-RLE) */
+    const uint32_t* shadow;      /* [N][shadow_words] */
+    int shadow_words;            /* must match the sky bins of the scene's sun positions */
+    int active_bins;
+} solar_gpu_lists;
+
+/* No counterpart in the reference (it always traces).  Stage 2/3 only: the
+   solar and reflection passes over caller-provided neighbor lists and shadow
+   words, for re-runs of a traced scene with new hourly irradiance (the sun
+   positions, and so the sky bins, must be the ones the lists were traced
+   with; shadow_words and active_bins are checked against them).  Scene
+   arrays are device pointers as for solar_gpu_run_device; lists are host
+   arrays.  opt->neighbor_format is ignored (lists->format is used).
+   Malformed lists cannot fault: offsets are checked on the host, ids outside
+   the top cells get weight 0, and ba-RLE decoding is bounds-checked
+   (SOLAR_GPU_ERR_DEVICE_CHECK). */
+int solar_gpu_run_lists(solar_gpu_context* ctx, const solar_gpu_options* opt, const solar_gpu_scene* scene,
+                        const solar_gpu_lists* lists, float* irradiance_out, void* stream);
+
 int solar_gpu_trace_copy(solar_gpu_context* ctx, long long* csr_offsets, int* csr_ids,
                          long long* barle_offsets, unsigned char* barle_bytes, uint32_t* shadow);
 

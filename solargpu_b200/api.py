@@ -52,6 +52,11 @@ class SceneDesc(C.Structure):
                 ("diffuse_irradiance", C.c_void_p), ("slopes", C.c_void_p), ("aspects", C.c_void_p)]
 
 
+class ListsDesc(C.Structure):
+    _fields_ = [("format", C.c_int), ("offsets", C.c_void_p), ("data", C.c_void_p), ("data_size", C.c_longlong),
+                ("shadow", C.c_void_p), ("shadow_words", C.c_int), ("active_bins", C.c_int)]
+
+
 _LIB = None
 
 
@@ -87,6 +92,7 @@ def lib() -> C.CDLL:
         L.solar_gpu_trace.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), vp]
         L.solar_gpu_trace_sizes.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.solar_gpu_trace_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.solar_gpu_run_lists.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), C.POINTER(ListsDesc), vp, vp]
         L.solar_gpu_last_timings.argtypes = [vp, C.POINTER(C.c_double), i]
         L.solar_gpu_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(ll), i]
         _LIB = L
@@ -237,6 +243,21 @@ class Context:
         o = options(**opts)
         d, keep = _scene_desc(scene, dev)
         _check(lib().solar_gpu_run_device(self.h, C.byref(o), C.byref(d), _p(out), stream))
+
+    def run_lists(self, scene, dev: dict, lists: dict, out, stream=None, **opts) -> None:
+        """Stage 2/3 over saved Stage 1 products (`lists`: a `trace()` result
+        or `cache.load_lists()`), scene arrays on the device as for
+        run_device.  The list format is the one `lists` holds (CSR first)."""
+        o = options(**opts)
+        d, keep = _scene_desc(scene, dev)
+        if "csr_off" in lists:
+            fmt, off, data = CSR, _host(lists["csr_off"], np.int64), _host(lists["csr_ids"], np.int32)
+        else:
+            fmt, off, data = BARLE, _host(lists["barle_off"], np.int64), _host(lists["barle"], np.uint8)
+        shadow = _host(lists["shadow"], np.uint32)
+        ld = ListsDesc(fmt, _p(off), _p(data) if data.size else None, int(data.size), _p(shadow),
+                       int(lists["shadow_words"]), int(lists["active_bins"]))
+        _check(lib().solar_gpu_run_lists(self.h, C.byref(o), C.byref(d), C.byref(ld), _p(out), stream))
 
     def trace(self, scene, dev: dict, neighbor_format: int = BOTH, stream=None, **opts) -> dict:
         """Runs Stage 1 and returns its lists and shadow words as numpy arrays."""

@@ -723,6 +723,69 @@ int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const sola
     return SOLAR_GPU_OK;
 }
 
+int run_lists_impl(solar_gpu_context* c, const solar_gpu_options* o_in, const solar_gpu_scene* s,
+                   const solar_gpu_lists* l, float* out, cudaStream_t st)
+{
+    if (!o_in || !l) return fail(SOLAR_GPU_ERR_ARG, "options or lists is NULL");
+    if (l->format != SOLAR_GPU_CSR && l->format != SOLAR_GPU_BARLE)
+        return fail(SOLAR_GPU_ERR_ARG, "lists format %d", l->format);
+    solar_gpu_options o = *o_in;
+    o.neighbor_format = l->format;
+    RK(check_scene(s));
+    RK(check_options(&o, false));
+    if (!out) return fail(SOLAR_GPU_ERR_ARG, "irradiance output is NULL");
+    const int N = s->num_total_voxels;
+    if (!l->offsets || !l->shadow || (l->data_size > 0 && !l->data) || l->data_size < 0)
+        return fail(SOLAR_GPU_ERR_ARG, "lists arrays are NULL");
+    if (l->offsets[0] != 0 || l->offsets[N] != l->data_size)
+        return fail(SOLAR_GPU_ERR_ARG, "list offsets run from %lld to %lld, data has %lld", l->offsets[0],
+                    l->offsets[N], l->data_size);
+    for (int v = 0; v < N; ++v)
+        if (l->offsets[v + 1] < l->offsets[v]) return fail(SOLAR_GPU_ERR_ARG, "list offsets decrease at voxel %d", v);
+    CK(cudaSetDevice(c->device));
+    c->launches = 0;
+    c->timed = false;
+    c->ktime = o.time_kernels != 0;
+    c->group_entries = 0;
+    c->staged_rows = 0;
+    c->weighted_entries = 0;
+    c->kt_used = 0;
+    c->kt_ids.clear();
+    c->kt_stream = st;
+    CK(cudaEventRecord(c->ev[0], st));
+    SkyTables sky;
+    RK(prepare(c, s, sky, st));
+    const int words32 = sky.words32 > 0 ? sky.words32 : 1;
+    if (l->shadow_words != words32 || l->active_bins != sky.active)
+        return fail(SOLAR_GPU_ERR_ARG, "lists were traced with %d sun bins (%d words), these sun positions give %d (%d)",
+                    l->active_bins, l->shadow_words, sky.active, words32);
+    CK(cudaEventRecord(c->ev[1], st));
+    c->N = N;
+    c->T = s->num_top_voxels;
+    c->words32 = words32;
+    c->active = sky.active;
+    c->have_csr = l->format == SOLAR_GPU_CSR;
+    c->have_barle = !c->have_csr;
+    c->csr_total = c->have_csr ? l->data_size : 0;
+    c->barle_total = c->have_barle ? l->data_size : 0;
+    RK(ensure(c->shadow, sizeof(uint32_t) * (size_t)N * words32));
+    CK(cudaMemcpyAsync(c->shadow.p, l->shadow, sizeof(uint32_t) * (size_t)N * words32, cudaMemcpyHostToDevice, st));
+    DevBuf& off = c->have_csr ? c->csr_off : c->barle_off;
+    DevBuf& dat = c->have_csr ? c->csr_ids : c->barle_bytes;
+    const size_t dbytes = (size_t)l->data_size * (c->have_csr ? sizeof(int) : 1);
+    RK(ensure(off, sizeof(long long) * ((size_t)N + 1)));
+    RK(ensure(dat, dbytes ? dbytes : 16));
+    CK(cudaMemcpyAsync(off.p, l->offsets, sizeof(long long) * ((size_t)N + 1), cudaMemcpyHostToDevice, st));
+    if (dbytes) CK(cudaMemcpyAsync(dat.p, l->data, dbytes, cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(c->ev[2], st));
+    RK(stage23(c, &o, s, sky, out, st));
+    CK(cudaEventRecord(c->ev[3], st));
+    CK(cudaStreamSynchronize(st));   // the host arrays may be released after return
+    RK(check_device_flags(c, st));
+    c->timed = true;
+    return SOLAR_GPU_OK;
+}
+
 std::mutex g_default_mu;
 solar_gpu_context* g_default = nullptr;
 
@@ -856,6 +919,13 @@ int solar_gpu_run_device(solar_gpu_context* c, const solar_gpu_options* o, const
     cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
     RK(run_device_impl(c, o, s, out, st, false));
     return check_device_flags(c, st);
+}
+
+int solar_gpu_run_lists(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
+                        const solar_gpu_lists* l, float* out, void* stream)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    return run_lists_impl(c, o, s, l, out, stream ? (cudaStream_t)stream : c->own);
 }
 
 int solar_gpu_run_host(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,

@@ -179,6 +179,39 @@ def test_tiles_equal_per_voxel_lists_on_barle(ctx, scene160, B):
     assert np.array_equal(outs[1], outs[2])
 
 
+@pytest.mark.parametrize("fmt", [0, 1])
+def test_run_from_cached_lists_with_new_tmy(ctx, scene160, fmt, tmp_path):
+    """Stage 1 saved to disk and re-run with other hourly irradiance gives the
+    same raster as a full run on that irradiance."""
+    import dataclasses
+    import torch
+    from solargpu_b200 import cache
+    s = scene160
+    dev = device_arrays(s)
+    p = str(tmp_path / "lists.npz")
+    cache.save_lists(p, ctx.trace(s, dev, neighbor_format=fmt), s, fmt=fmt)
+    s2 = dataclasses.replace(s, direct=(s.direct * np.float32(0.7)), diffuse=(s.diffuse * np.float32(1.3)))
+    want = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
+    ctx.run_device(s2, dev, want, neighbor_format=fmt)
+    got = torch.zeros_like(want)
+    ctx.run_lists(s2, dev, cache.load_lists(p, s2), got)
+    torch.cuda.synchronize()
+    assert np.array_equal(got.cpu().numpy(), want.cpu().numpy())
+    assert rel_err(got.cpu().numpy(), fp64_reference(s2)).max() <= REL_TOL
+
+
+def test_run_lists_rejects_other_sky_bins(ctx, scene64):
+    import torch
+    from solargpu_b200 import api
+    dev = device_arrays(scene64)
+    r = ctx.trace(scene64, dev, neighbor_format=0)
+    r["active_bins"] += 1
+    out = torch.zeros(scene64.num_total, dtype=torch.float32, device="cuda:0")
+    with pytest.raises(api.SolarGPUError) as e:
+        ctx.run_lists(scene64, dev, r, out)
+    assert e.value.code == -1
+
+
 def test_invalid_hour_block_for_group_is_rejected(ctx, scene64):
     import torch
     from solargpu_b200 import api

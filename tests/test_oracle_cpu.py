@@ -156,3 +156,35 @@ def test_fp64_oracle_matches_reference_annual_output(name):
         rel = np.abs(g[key].astype(np.float64) - tot) / tot
         assert rel.max() < 2e-5, (key, rel.max())
         assert rel.mean() < 2e-6, (key, rel.mean())
+
+
+def test_lists_cache_roundtrip_and_fingerprints(tmp_path):
+    """The on-disk Stage 1 cache keeps the lists exactly and refuses scenes
+    whose geometry or sun positions differ from the traced one."""
+    import dataclasses
+    from solargpu_b200 import cache
+    s = load_scene("dsm64")
+    bins, off, ids, sh = oracle_trace(s)
+    r = {"csr_off": off.astype(np.int64), "csr_ids": ids.astype(np.int32), "shadow": sh,
+         "shadow_words": sh.shape[1], "active_bins": bins["active"]}
+    p = str(tmp_path / "t.npz")
+    cache.save_lists(p, r, s)
+    got = cache.load_lists(p, s)
+    assert np.array_equal(got["csr_off"], r["csr_off"]) and np.array_equal(got["csr_ids"], r["csr_ids"])
+    assert np.array_equal(got["shadow"], sh) and got["active_bins"] == bins["active"]
+    # new hourly irradiance: same fingerprints
+    s2 = dataclasses.replace(s, direct=s.direct * np.float32(0.5))
+    cache.load_lists(p, s2)
+    s3 = dataclasses.replace(s, grid=s.grid + np.float32(1.0))
+    with pytest.raises(ValueError):
+        cache.load_lists(p, s3)
+    sun = s.sun.copy()
+    sun[100:200, 0] += np.float32(1.0)
+    with pytest.raises(ValueError):
+        cache.load_lists(p, dataclasses.replace(s, sun=sun))
+    from oracle import oracle as O
+    boff, bbytes = O.barle_encode_csr(off, ids)
+    rb = {"barle_off": boff, "barle": bbytes, "shadow": sh, "shadow_words": sh.shape[1], "active_bins": bins["active"]}
+    cache.save_lists(p, rb, s)
+    gb = cache.load_lists(p)
+    assert np.array_equal(gb["barle"], bbytes) and "csr_off" not in gb
