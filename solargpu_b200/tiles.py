@@ -13,8 +13,9 @@ Worker threads each own a context and a CUDA stream, so the small tiles of
 one worker overlap the host-side set-up and launches of another (the ctypes
 calls release the GIL).  The autotuner times each candidate configuration
 (list format x hour block x reflection kernel) on the first tile of a size
-bucket (log2 of the voxel count) and reuses the fastest for the bucket; the
-table can be saved and reloaded as JSON.
+bucket (log2 of the voxel count), alone on the GPU before the workers start,
+and reuses the fastest for the bucket; the table can be saved and reloaded
+as JSON.
 """
 from __future__ import annotations
 
@@ -71,7 +72,8 @@ class Autotuner:
 
     def choose(self, bucket: int, measure) -> dict:
         """measure(params) -> milliseconds; called for each candidate the
-        first time a bucket is seen."""
+        first time a bucket is seen (measure may be None once every bucket
+        in use has been tuned)."""
         with self.lock:
             if bucket in self.table:
                 return self.table[bucket]
@@ -109,19 +111,31 @@ def run_tiles(scenes: list, params: dict | None = None, tuner: Autotuner | None 
     results: list = [None] * len(scenes)
     errors: list = []
 
+    if tuner is not None:
+        # Tuning runs first, alone on the GPU (one context, one stream), on
+        # the first tile of each size bucket: the median of 3 timed runs of
+        # each candidate after an untimed one.
+        stream = torch.cuda.Stream(device=dev)
+        with api.Context(device) as ctx:
+            for s, d, out in staged:
+                def measure(c):
+                    ctx.run_device(s, d, out, stream=stream.cuda_stream, accumulation=accumulation, **c)
+                    ms = []
+                    for _ in range(3):
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        ctx.run_device(s, d, out, stream=stream.cuda_stream, accumulation=accumulation, **c)
+                        e1.record(stream)
+                        e1.synchronize()
+                        ms.append(e0.elapsed_time(e1))
+                    return sorted(ms)[1]
+                tuner.choose(size_bucket(s), measure)
+
     def run_one(ctx, stream, i, timed):
         s, d, out = staged[i]
         p = dict(params or DEFAULT)
         if tuner is not None:
-            def measure(c):
-                ctx.run_device(s, d, out, stream=stream.cuda_stream, accumulation=accumulation, **c)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                ctx.run_device(s, d, out, stream=stream.cuda_stream, accumulation=accumulation, **c)
-                e1.record(stream)
-                e1.synchronize()
-                return e0.elapsed_time(e1)
-            p = tuner.choose(size_bucket(s), measure)
+            p = tuner.choose(size_bucket(s), None)
         if not timed:
             ctx.run_device(s, d, out, stream=stream.cuda_stream, accumulation=accumulation, **p)
             return
