@@ -565,20 +565,31 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
             const unsigned short* rv = reinterpret_cast<const unsigned short*>(st + L::kRow);
             const int* tab = reinterpret_cast<const int*>(st + L::kTab);
             const int b = tab[warp], e = tab[warp + 1];
+            // A zero weight (a voxel of the quad without this neighbor) adds
+            // an exact +0 to nonnegative sums, so its FMAs are skipped; the
+            // weights are the same in all lanes, so the branches are uniform.
 #pragma unroll 2
             for (int i = b; i < e; ++i) {
                 const int r = rv[i];
                 const float4 w = wv[i];
                 float x[Q];
                 smem_row<Q>(x, rows + r * kRowFloats, lane);
+                if (w.x != 0.0f) {
 #pragma unroll
-                for (int h = 0; h < Q; ++h) a[0][h] = fmaf(w.x, x[h], a[0][h]);
+                    for (int h = 0; h < Q; ++h) a[0][h] = fmaf(w.x, x[h], a[0][h]);
+                }
+                if (w.y != 0.0f) {
 #pragma unroll
-                for (int h = 0; h < Q; ++h) a[1][h] = fmaf(w.y, x[h], a[1][h]);
+                    for (int h = 0; h < Q; ++h) a[1][h] = fmaf(w.y, x[h], a[1][h]);
+                }
+                if (w.z != 0.0f) {
 #pragma unroll
-                for (int h = 0; h < Q; ++h) a[2][h] = fmaf(w.z, x[h], a[2][h]);
+                    for (int h = 0; h < Q; ++h) a[2][h] = fmaf(w.z, x[h], a[2][h]);
+                }
+                if (w.w != 0.0f) {
 #pragma unroll
-                for (int h = 0; h < Q; ++h) a[3][h] = fmaf(w.w, x[h], a[3][h]);
+                    for (int h = 0; h < Q; ++h) a[3][h] = fmaf(w.w, x[h], a[3][h]);
+                }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&bar_empty[s]));
