@@ -232,3 +232,36 @@ def test_invalid_pixel_parent_is_rejected(ctx, scene64):
         ctx.run_device(scene64, dev, out)
     assert e.value.code == -1
     ctx.run_device(scene64, device_arrays(scene64), out)   # the context stays usable
+
+
+def _edge_scene(kind):
+    """Degenerate scenes: a flat field (no walls, nearly empty lists), a lone
+    tower (a few wall voxels with long lists next to many empty ones) and a
+    7 x 5 strip whose voxel count is no multiple of 4 or 64."""
+    from solargpu_b200 import inputs
+    if kind == "flat":
+        z = np.zeros((24, 24), np.float32)
+    elif kind == "tower":
+        z = np.zeros((32, 32), np.float32)
+        z[14:17, 14:17] = 25.0
+    else:
+        z = np.zeros((5, 7), np.float32)
+        z[2, 3] = 3.0
+    cfg = inputs.DsmConfig(f"edge_{kind}", z.shape[1], 0, 0, seed=5)
+    return inputs.make_scene(cfg, heights=z)
+
+
+@pytest.mark.parametrize("kind", ["flat", "tower", "strip"])
+@pytest.mark.parametrize("fmt,B,V", [(0, 256, 64), (1, 256, 64), (0, 128, 64), (1, 128, 1), (0, 1, 0)])
+def test_degenerate_scenes(ctx, kind, fmt, B, V):
+    import torch
+    s = _edge_scene(kind)
+    out = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
+    ctx.run_device(s, device_arrays(s), out, neighbor_format=fmt, hour_block=B, group_size=V, accumulation=1)
+    torch.cuda.synchronize()
+    e = rel_err(out.cpu().numpy(), fp64_reference(s))
+    assert e.max() <= REL_TOL, (e.max(), e.mean())
+    r = ctx.trace(s, device_arrays(s), neighbor_format=2)
+    bins, off, ids, sh = oracle_trace(s)
+    assert np.array_equal(r["csr_off"], off) and np.array_equal(r["csr_ids"], ids)
+    assert np.array_equal(r["shadow"], sh)
