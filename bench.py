@@ -57,7 +57,10 @@ def parse():
 # ---------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) of SM clock and throttle reasons while running."""
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons.  Started
+    before the warm-up (nvidia-smi's own start-up slows the GPU's host side
+    for a few hundred ms); mark() opens the timed region, stop() closes it and
+    summarises the samples taken in between."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -66,6 +69,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines: list[str] = []
+        self.first = 0
 
     def start(self):
         try:
@@ -81,6 +85,15 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_ready(self, samples: int = 3, timeout_s: float = 5.0):
+        """Returns once nvidia-smi has delivered a few samples (past its start-up)."""
+        t0 = time.perf_counter()
+        while self.proc is not None and len(self.lines) < samples and time.perf_counter() - t0 < timeout_s:
+            time.sleep(0.05)
+
+    def mark(self):
+        self.first = len(self.lines)
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -91,7 +104,8 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
+        timed = self.lines[self.first:] or self.lines
+        for ln in timed:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -211,13 +225,15 @@ def run_ours(args, world, rank, local, pg):
     def step():
         ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
 
+    sampler = ClockSampler(local)
+    sampler.start()
+    sampler.wait_ready()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
 
     # ---- timed region
-    sampler = ClockSampler(local)
-    sampler.start()
+    sampler.mark()
     barrier(pg)
     torch.cuda.synchronize(dev)
     evs = []
