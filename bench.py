@@ -124,15 +124,19 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- helpers
 
-def dist_setup(args):
+def dist_setup(args=None, backend: str | None = None):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo without (tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pg = None
     if world > 1:
         import datetime
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
 
@@ -143,12 +147,20 @@ def barrier(pg):
 
 
 def max_over_ranks(pg, x: float, device) -> float:
+    """The slowest rank's time (every rank gets it)."""
     if pg is None:
         return x
     import torch
+    if pg.get_backend() == "gloo":
+        device = "cpu"
     t = torch.tensor([x], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_rate(world: int, units_per_rank: float, steps: int, slowest_ms: float) -> float:
+    """Whole-job rate: every rank's units over the slowest rank's time."""
+    return world * units_per_rank * steps / (slowest_ms / 1e3)
 
 
 _PINNED = []
@@ -264,7 +276,7 @@ def run_ours(args, world, rank, local, pg):
     api.lib().solar_gpu_trace_sizes(ctx.h, C.byref(ne), C.byref(nb), C.byref(w), C.byref(a_), C.byref(n_))
     Hd = int(((scene.sun[:, 1] - np.float32(1e-8)) >= 1.0).sum())
     units = float(N) * Hd
-    value = world * units * args.steps / (total_ms / 1e3)
+    value = aggregate_rate(world, units, args.steps, total_ms)
     ms_per_step = total_ms / args.steps
 
     # ---- dominant kernel roofline (live events over the timed region)
