@@ -222,6 +222,16 @@ long long solar_gpu_last_weighted_entries(solar_gpu_context* ctx);
 /* Number of kernel launches the library issued in the last run. */
 long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
 
+/* ---- tensor-core GEMM (sky-bin visibility surrogate) ------------------- */
+
+/* No counterpart in the reference.  C[M][N] = A[M][K] x B[N][K]^T (+ bias[N],
+   ReLU if relu != 0) on the tcgen05 tensor cores: A, B bf16 row-major (K
+   contiguous), f32 accumulation in TMEM, output f32 (C) and/or bf16 (C_bf16),
+   row-major; device pointers, 16-byte aligned.  M and N multiples of 128, K a
+   multiple of 64.  Synchronous on `stream`. */
+int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N,
+                        int K, int relu, void* stream);
+
 /* ---- encoding without device allocation -------------------------------- */
 
 /* No counterpart in the reference.  ba-RLE-encodes num_lists CSR neighbor

@@ -93,6 +93,7 @@ def lib() -> C.CDLL:
         L.solar_gpu_trace_sizes.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.solar_gpu_trace_copy.argtypes = [vp, vp, vp, vp, vp, vp]
         L.solar_gpu_run_lists.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), C.POINTER(ListsDesc), vp, vp]
+        L.solar_gpu_gemm_bf16.argtypes = [vp, vp, vp, vp, vp, i, i, i, i, vp]
         L.solar_gpu_last_timings.argtypes = [vp, C.POINTER(C.c_double), i]
         L.solar_gpu_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(ll), i]
         _LIB = L
@@ -171,6 +172,18 @@ def compressed_gpu_irradiance(grid_data, grid_width, grid_height, num_total_voxe
 
 
 # ---------------------------------------------------------------- context
+
+def gemm_bf16(A, B, out=None, out_bf16=None, bias=None, relu: bool = False, stream=None):
+    """C = A @ B.T (+ bias, ReLU) on the tensor cores; A [M, K], B [N, K]
+    bf16 CUDA tensors (contiguous), M and N multiples of 128, K of 64."""
+    import torch
+    M, K = A.shape
+    N = B.shape[0]
+    if out is None and out_bf16 is None:
+        out = torch.empty(M, N, dtype=torch.float32, device=A.device)
+    _check(lib().solar_gpu_gemm_bf16(_p(A), _p(B), _p(out), _p(out_bf16), _p(bias), M, N, K, int(relu), stream))
+    return out if out is not None else out_bf16
+
 
 def _scene_desc(scene, dev: dict | None = None) -> tuple[SceneDesc, list]:
     """Builds the C scene struct.  With `dev`, the per-voxel arrays come from
