@@ -222,6 +222,13 @@ long long solar_gpu_last_weighted_entries(solar_gpu_context* ctx);
 /* Number of kernel launches the library issued in the last run. */
 long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
 
+/* No counterpart in the reference.  The sun-bin shadow words of the listed
+   voxels only (device int32 ids, at most 2^20), traced exactly as the full
+   pass traces them; out is device [n][*shadow_words].  Used to spot-check
+   and to fall back from the visibility surrogate. */
+int solar_gpu_trace_shadow_subset(solar_gpu_context* ctx, const solar_gpu_scene* scene, const int* voxels, int n,
+                                  uint32_t* shadow_out, int* shadow_words, void* stream);
+
 /* ---- tensor-core GEMM (sky-bin visibility surrogate) ------------------- */
 
 /* No counterpart in the reference.  C[M][N] = A[M][K] x B[N][K]^T (+ bias[N],
@@ -231,6 +238,29 @@ long long solar_gpu_last_launch_count(solar_gpu_context* ctx);
    multiple of 64.  Synchronous on `stream`. */
 int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N,
                         int K, int relu, void* stream);
+
+/* Surrogate training/inference kernels (device pointers, bf16 = 2-byte
+   bfloat16, row-major).  features: per voxel the 64 x 64 heights around its
+   pixel relative to its base height / 50 m (clipped to +-2) and its normal,
+   zero-padded to feat (>= 4099) columns.  labels: the first `active` shadow
+   bits of each voxel as 0/1 floats over outw columns.  bce: mean binary
+   cross-entropy with logits over the first `active` columns (adds to *loss),
+   dZ = (sigmoid(Z) - Y) / (M active) as bf16.  relu_grad: dX = dY (H > 0).
+   transpose: out[C][R] = in[R][C].  colsum: out[c] = sum_r in[r][c].  adam:
+   one Adam step on FP32 parameters (bias-corrected, step >= 1), optional
+   bf16 copy. */
+int solar_gpu_sg_features(const float* grid, int W, int H, int T, const int* pixel_parent, const float* wall_z,
+                          const float* slopes, const float* aspects, const int* voxels, int M, int feat,
+                          void* out_bf16, void* stream);
+int solar_gpu_sg_labels(const uint32_t* shadow, int words32, const int* voxels, int M, int active, int outw,
+                        float* y, void* stream);
+int solar_gpu_sg_bce(const float* Z, const float* Y, int M, int outw, int active, void* dZ_bf16, float* loss,
+                     void* stream);
+int solar_gpu_sg_relu_grad(const float* dY, const void* H_bf16, long long n, void* dX_bf16, void* stream);
+int solar_gpu_sg_transpose(const void* in_bf16, int R, int C, void* out_bf16, void* stream);
+int solar_gpu_sg_colsum(const void* in_bf16, int R, int C, float* out, void* stream);
+int solar_gpu_sg_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                      float eps, int step, void* p_bf16, void* stream);
 
 /* ---- encoding without device allocation -------------------------------- */
 

@@ -58,6 +58,12 @@ struct DevBuf {
 template <typename T> T* as(DevBuf& b) { return static_cast<T*>(b.p); }
 
 
+__global__ void k_check_ids(const int* __restrict__ ids, int n, int N, int* __restrict__ bad)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && (unsigned)ids[i] >= (unsigned)N) atomicOr(bad, 1);
+}
+
 __global__ void k_validate_parents(const int* __restrict__ pp, int N, int T, int* __restrict__ bad)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -786,6 +792,49 @@ int run_lists_impl(solar_gpu_context* c, const solar_gpu_options* o_in, const so
     return SOLAR_GPU_OK;
 }
 
+__global__ void k_gather_shadow(const uint32_t* __restrict__ shadow, int words32, const int* __restrict__ voxels,
+                                int n, uint32_t* __restrict__ out)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < (long long)n * words32) out[t] = shadow[(size_t)voxels[t / words32] * words32 + t % words32];
+}
+
+int trace_subset_impl(solar_gpu_context* c, const solar_gpu_scene* s, const int* voxels, int n, uint32_t* out,
+                      int* words_out, cudaStream_t st)
+{
+    RK(check_scene(s));
+    if (!voxels || !out || n < 0) return fail(SOLAR_GPU_ERR_ARG, "voxels / output is NULL");
+    if (n > (1 << 20)) return fail(SOLAR_GPU_ERR_ARG, "at most %d voxels per call (got %d)", 1 << 20, n);
+    CK(cudaSetDevice(c->device));
+    c->launches = 0;
+    c->ktime = false;
+    SkyTables sky;
+    RK(prepare(c, s, sky, st));
+    const int N = s->num_total_voxels, D = (int)sky.dirs.size();
+    const int words32 = sky.words32 > 0 ? sky.words32 : 1;
+    if (words_out) *words_out = words32;
+    if (n == 0) return SOLAR_GPU_OK;
+    // the listed voxels must exist (the tracer reads their parents)
+    RK(ensure(c->err, sizeof(int)));
+    RK(ensure(c->shadow, sizeof(uint32_t) * (size_t)N * words32));
+    CK(cudaMemsetAsync(c->shadow.p, 0, sizeof(uint32_t) * (size_t)N * words32, st));
+    RK(ensure(c->raw, sizeof(int) * (size_t)n * D));
+    RK(ensure(c->order_inv, sizeof(int) * (size_t)n));
+    k_check_ids<<<(n + 255) / 256, 256, 0, st>>>(voxels, n, N, as<int>(c->err));
+    CK(cudaMemcpyAsync(c->h_scalars, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int bad = 0;
+    std::memcpy(&bad, c->h_scalars, sizeof(int));
+    if (bad) return fail(SOLAR_GPU_ERR_ARG, "voxel ids outside [0, %d)", N);
+    CK(launch_trace(dev_scene(s), as<DirEntry>(c->dirs), D, words32, 0, n, as<int>(c->raw),
+                    as<uint32_t>(c->shadow), voxels, st));
+    const long long cells = (long long)n * words32;
+    k_gather_shadow<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(as<uint32_t>(c->shadow), words32, voxels, n, out);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return SOLAR_GPU_OK;
+}
+
 std::mutex g_default_mu;
 solar_gpu_context* g_default = nullptr;
 
@@ -926,6 +975,13 @@ int solar_gpu_run_lists(solar_gpu_context* c, const solar_gpu_options* o, const 
 {
     if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
     return run_lists_impl(c, o, s, l, out, stream ? (cudaStream_t)stream : c->own);
+}
+
+int solar_gpu_trace_shadow_subset(solar_gpu_context* c, const solar_gpu_scene* s, const int* voxels, int n,
+                                  uint32_t* shadow_out, int* shadow_words, void* stream)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    return trace_subset_impl(c, s, voxels, n, shadow_out, shadow_words, stream ? (cudaStream_t)stream : c->own);
 }
 
 int solar_gpu_run_host(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,

@@ -22,6 +22,9 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <cmath>
+
 namespace sgb {
 namespace {
 
@@ -193,6 +196,125 @@ k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTn));
 }
 
+// ---- surrogate training and inference kernels ------------------------------
+
+constexpr int kPatch = 64;             // height patch side (cells) around the voxel's pixel
+constexpr float kPatchScale = 1.0f / 50.0f;
+
+// Features of voxel voxels[i]: the 64 x 64 heights around its pixel relative
+// to the voxel's base height, / 50 m, clipped to [-2, 2] (outside the grid:
+// ground at 0 m), then the voxel normal; zero padding up to `feat`.
+__global__ void k_sg_features(const float* __restrict__ grid, int W, int H, int T, const int* __restrict__ pp,
+                              const float* __restrict__ wall_z, const float* __restrict__ slopes,
+                              const float* __restrict__ aspects, const int* __restrict__ voxels, int M, int feat,
+                              __nv_bfloat16* __restrict__ out)
+{
+    const int i = blockIdx.y;
+    if (i >= M) return;
+    const int v = voxels[i];
+    const int top = pp[v];
+    const int gx = top % W, gy = top / W;
+    const float z = v < T ? grid[top] : wall_z[v - T];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < feat; j += gridDim.x * blockDim.x) {
+        float f = 0.0f;
+        if (j < kPatch * kPatch) {
+            const int x = gx + (j % kPatch) - kPatch / 2, y = gy + (j / kPatch) - kPatch / 2;
+            const float h = (x >= 0 && x < W && y >= 0 && y < H) ? grid[y * W + x] : 0.0f;
+            f = fminf(2.0f, fmaxf(-2.0f, (h - z) * kPatchScale));
+        } else if (j < kPatch * kPatch + 3) {
+            const float sl = slopes[v] * 0.017453292f, as = aspects[v] * 0.017453292f;
+            const int c = j - kPatch * kPatch;
+            f = c == 0 ? sinf(sl) * sinf(as) : c == 1 ? -sinf(sl) * cosf(as) : cosf(sl);
+        }
+        out[(size_t)i * feat + j] = __float2bfloat16_rn(f);
+    }
+}
+
+// Labels: bit b (< active) of voxels[i]'s shadow words -> 1.0 (shadowed) / 0.0.
+__global__ void k_sg_labels(const uint32_t* __restrict__ shadow, int words32, const int* __restrict__ voxels, int M,
+                            int active, int outw, float* __restrict__ y)
+{
+    const int i = blockIdx.x, b = threadIdx.x;
+    if (i >= M) return;
+    const int v = voxels[i];
+    for (int k = b; k < outw; k += blockDim.x)
+        y[(size_t)i * outw + k] = k < active ? (float)((shadow[(size_t)v * words32 + (k >> 5)] >> (k & 31)) & 1u) : 0.0f;
+}
+
+// Mean binary cross-entropy with logits over the first `active` outputs:
+// dZ = (sigmoid(Z) - Y) / (M * active) as bf16, loss sum into *loss.
+__global__ void k_sg_bce(const float* __restrict__ Z, const float* __restrict__ Y, int M, int outw, int active,
+                         __nv_bfloat16* __restrict__ dZ, float* __restrict__ loss)
+{
+    const long long n = (long long)M * outw;
+    const float inv = 1.0f / ((float)M * (float)active);
+    float part = 0.0f;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % outw);
+        float g = 0.0f;
+        if (k < active) {
+            const float z = Z[t], y = Y[t];
+            const float p = 1.0f / (1.0f + expf(-z));
+            g = (p - y) * inv;
+            part += fmaxf(z, 0.0f) - z * y + log1pf(expf(-fabsf(z)));
+        }
+        dZ[t] = __float2bfloat16_rn(g);
+    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, part * inv);
+}
+
+// dX = dY * (H > 0) as bf16 (ReLU backward through a stored activation).
+__global__ void k_sg_relu_grad(const float* __restrict__ dY, const __nv_bfloat16* __restrict__ H, long long n,
+                               __nv_bfloat16* __restrict__ dX)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        dX[t] = __float2bfloat16_rn(__bfloat162float(H[t]) > 0.0f ? dY[t] : 0.0f);
+}
+
+// out[c][r] = in[r][c] (bf16, 32 x 32 tiles through shared memory).
+__global__ void k_sg_transpose(const __nv_bfloat16* __restrict__ in, int R, int C, __nv_bfloat16* __restrict__ out)
+{
+    __shared__ __nv_bfloat16 t[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r < R && c < C) t[k][threadIdx.x] = in[(size_t)r * C + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < R && c < C) out[(size_t)c * R + r] = t[threadIdx.x][k];
+    }
+}
+
+// out[c] = sum over rows of in[r][c] (bias gradients).
+__global__ void k_sg_colsum(const __nv_bfloat16* __restrict__ in, int R, int C, float* __restrict__ out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    float s = 0.0f;
+    for (int r = 0; r < R; ++r) s += __bfloat162float(in[(size_t)r * C + c]);
+    out[c] = s;
+}
+
+// Adam on FP32 master parameters; the bf16 copy feeds the GEMMs.
+__global__ void k_sg_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
+                          float c2, __nv_bfloat16* __restrict__ pb)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const float gt = g[t];
+        const float mt = b1 * m[t] + (1.0f - b1) * gt;
+        const float vt = b2 * v[t] + (1.0f - b2) * gt * gt;
+        m[t] = mt;
+        v[t] = vt;
+        const float q = p[t] - lr * (mt / c1) / (sqrtf(vt / c2) + eps);
+        p[t] = q;
+        if (pb) pb[t] = __float2bfloat16_rn(q);
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, const float* bias, int M, int N,
@@ -209,6 +331,82 @@ cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, c
 }  // namespace sgb
 
 extern "C" {
+
+namespace {
+int sg_status(cudaError_t e)
+{
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        sgb::set_last_error(cudaGetErrorString(e));
+        return -2;
+    }
+    return 0;
+}
+unsigned sg_blocks(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16); }
+}  // namespace
+
+int solar_gpu_sg_features(const float* grid, int W, int H, int T, const int* pixel_parent, const float* wall_z,
+                          const float* slopes, const float* aspects, const int* voxels, int M, int feat,
+                          void* out_bf16, void* stream)
+{
+    if (M <= 0) return 0;
+    if (feat < 4096 + 3 || M > 65535) { sgb::set_last_error("features: feat >= 4099, M <= 65535"); return -1; }
+    sgb::k_sg_features<<<dim3(4, M), 256, 0, (cudaStream_t)stream>>>(grid, W, H, T, pixel_parent, wall_z, slopes,
+                                                                     aspects, voxels, M, feat,
+                                                                     (__nv_bfloat16*)out_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_labels(const uint32_t* shadow, int words32, const int* voxels, int M, int active, int outw,
+                        float* y, void* stream)
+{
+    if (M <= 0) return 0;
+    if (active > outw || active > 32 * words32) { sgb::set_last_error("labels: active bins"); return -1; }
+    sgb::k_sg_labels<<<M, 128, 0, (cudaStream_t)stream>>>(shadow, words32, voxels, M, active, outw, y);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_bce(const float* Z, const float* Y, int M, int outw, int active, void* dZ_bf16, float* loss,
+                     void* stream)
+{
+    const long long n = (long long)M * outw;
+    if (n <= 0) return 0;
+    sgb::k_sg_bce<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>(Z, Y, M, outw, active, (__nv_bfloat16*)dZ_bf16, loss);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_relu_grad(const float* dY, const void* H_bf16, long long n, void* dX_bf16, void* stream)
+{
+    if (n <= 0) return 0;
+    sgb::k_sg_relu_grad<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>(dY, (const __nv_bfloat16*)H_bf16, n,
+                                                                        (__nv_bfloat16*)dX_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_transpose(const void* in_bf16, int R, int C, void* out_bf16, void* stream)
+{
+    if (R <= 0 || C <= 0) return 0;
+    sgb::k_sg_transpose<<<dim3((C + 31) / 32, (R + 31) / 32), dim3(32, 8), 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)in_bf16, R, C, (__nv_bfloat16*)out_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_colsum(const void* in_bf16, int R, int C, float* out, void* stream)
+{
+    if (R <= 0 || C <= 0) return 0;
+    sgb::k_sg_colsum<<<(C + 127) / 128, 128, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in_bf16, R, C, out);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                      float eps, int step, void* p_bf16, void* stream)
+{
+    if (n <= 0) return 0;
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    sgb::k_sg_adam<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2,
+                                                                  (__nv_bfloat16*)p_bf16);
+    return sg_status(cudaSuccess);
+}
 
 int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N,
                         int K, int relu, void* stream)

@@ -1,0 +1,240 @@
+"""Sky-bin visibility surrogate: a BF16 MLP on the tcgen05 GEMM.
+
+For a voxel, the model predicts its 265 sun-bin shadow bits (the DDA's
+shadow words: 1 = a ray toward that bin hits terrain) from the 64 x 64
+heights around its pixel (relative to the voxel's base height, / 50 m) and
+its normal:
+
+    features (4099, zero-padded to 4224) -> 512 -> 512 -> 512 -> 384 logits
+    (the first `active` columns are the sun bins), ReLU between layers.
+
+Every matrix product, forward and backward, runs on the tensor cores through
+`solar_gpu_gemm_bf16` (bf16 operands, f32 accumulation in TMEM); features,
+labels, the loss, ReLU backward, transposes, bias sums and Adam are small
+CUDA kernels of the library.  Master weights and Adam moments are FP32,
+the GEMMs read bf16 copies.
+
+`predict_with_fallback` is the guarded use: bits for every voxel from the
+model, then per 256 x 256-cell tile a random sample of voxels traced exactly
+(`solar_gpu_trace_shadow_subset`); a tile whose sampled bit error exceeds the
+threshold (2%) is traced exactly in full.  The result is exact on fallback
+tiles and within the sampled error elsewhere.  The model does not predict the
+reflected share; reflection needs the exact neighbor lists.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import api
+
+FEAT = 4224      # 64 * 64 + 3, padded to a multiple of 128
+OUTW = 384       # >= 265 active sun bins, a multiple of 128
+
+
+def _lib():
+    L = api.lib()
+    if not getattr(L, "_sg_bound", False):
+        vp, i, f, ll = C.c_void_p, C.c_int, C.c_float, C.c_longlong
+        L.solar_gpu_sg_features.argtypes = [vp, i, i, i, vp, vp, vp, vp, vp, i, i, vp, vp]
+        L.solar_gpu_sg_labels.argtypes = [vp, i, vp, i, i, i, vp, vp]
+        L.solar_gpu_sg_bce.argtypes = [vp, vp, i, i, i, vp, vp, vp]
+        L.solar_gpu_sg_relu_grad.argtypes = [vp, vp, ll, vp, vp]
+        L.solar_gpu_sg_transpose.argtypes = [vp, i, i, vp, vp]
+        L.solar_gpu_sg_colsum.argtypes = [vp, i, i, vp, vp]
+        L.solar_gpu_sg_adam.argtypes = [vp, vp, vp, vp, ll, f, f, f, f, i, vp, vp]
+        L.solar_gpu_trace_shadow_subset.argtypes = [vp, C.POINTER(api.SceneDesc), vp, i, vp, C.POINTER(i), vp]
+        L._sg_bound = True
+    return L
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(int(t.data_ptr()))
+
+
+def _t(torch, x):
+    """Transpose of a 2-D bf16 CUDA tensor through the library kernel."""
+    R, Cc = x.shape
+    out = torch.empty(Cc, R, dtype=torch.bfloat16, device=x.device)
+    api._check(_lib().solar_gpu_sg_transpose(_p(x), R, Cc, _p(out), None))
+    return out
+
+
+class Surrogate:
+    def __init__(self, active: int, hidden: int = 512, layers: int = 3, feat: int = FEAT, outw: int = OUTW,
+                 seed: int = 0, device: int = 0):
+        import torch
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.active, self.feat, self.outw = active, feat, outw
+        self.dims = [feat] + [hidden] * layers + [outw]
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        self.W, self.b = [], []
+        for a, o in zip(self.dims[:-1], self.dims[1:]):
+            self.W.append((torch.randn(o, a, generator=g) * math.sqrt(2.0 / a)).to(self.dev))
+            self.b.append(torch.zeros(o, device=self.dev))
+        self.Wb = [w.to(torch.bfloat16) for w in self.W]
+        self.mW = [torch.zeros_like(w) for w in self.W]
+        self.vW = [torch.zeros_like(w) for w in self.W]
+        self.mb = [torch.zeros_like(b) for b in self.b]
+        self.vb = [torch.zeros_like(b) for b in self.b]
+        self.step_count = 0
+
+    # -- data -----------------------------------------------------------------
+
+    def features(self, scene, dev: dict, voxels):
+        torch = self.torch
+        M = voxels.numel()
+        out = torch.empty(M, self.feat, dtype=torch.bfloat16, device=self.dev)
+        api._check(_lib().solar_gpu_sg_features(_p(dev["grid"]), scene.width, scene.height, scene.num_top,
+                                                _p(dev["pixel_parent"]), _p(dev["wall_z"]), _p(dev["slopes"]),
+                                                _p(dev["aspects"]), _p(voxels), M, self.feat, _p(out), None))
+        return out
+
+    def labels(self, shadow_dev, words32: int, voxels):
+        torch = self.torch
+        M = voxels.numel()
+        y = torch.empty(M, self.outw, dtype=torch.float32, device=self.dev)
+        api._check(_lib().solar_gpu_sg_labels(_p(shadow_dev), words32, _p(voxels), M, self.active, self.outw,
+                                              _p(y), None))
+        return y
+
+    # -- model ----------------------------------------------------------------
+
+    def forward(self, X):
+        """Activations (bf16, ReLU applied) of every hidden layer and the f32 logits."""
+        torch = self.torch
+        acts = [X]
+        h = X
+        for l in range(len(self.Wb) - 1):
+            hn = torch.empty(h.shape[0], self.dims[l + 1], dtype=torch.bfloat16, device=self.dev)
+            api.gemm_bf16(h, self.Wb[l], out_bf16=hn, bias=self.b[l], relu=True)
+            acts.append(hn)
+            h = hn
+        Z = api.gemm_bf16(h, self.Wb[-1], bias=self.b[-1])
+        return acts, Z
+
+    def gradients(self, X, Y):
+        """Loss and the gradients of every weight and bias (f32)."""
+        torch = self.torch
+        M = X.shape[0]
+        acts, Z = self.forward(X)
+        loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
+        g = torch.empty(M, self.outw, dtype=torch.bfloat16, device=self.dev)
+        api._check(_lib().solar_gpu_sg_bce(_p(Z), _p(Y), M, self.outw, self.active, _p(g), _p(loss), None))
+        dW = [None] * len(self.W)
+        db = [None] * len(self.W)
+        for l in range(len(self.W) - 1, -1, -1):
+            a = acts[l]
+            dW[l] = api.gemm_bf16(_t(torch, g), _t(torch, a))                 # [out, in] = g^T a
+            db[l] = torch.empty(self.dims[l + 1], dtype=torch.float32, device=self.dev)
+            api._check(_lib().solar_gpu_sg_colsum(_p(g), M, self.dims[l + 1], _p(db[l]), None))
+            if l > 0:
+                dA = api.gemm_bf16(g, _t(torch, self.Wb[l]))                  # [M, in] = g W
+                gn = torch.empty(M, self.dims[l], dtype=torch.bfloat16, device=self.dev)
+                api._check(_lib().solar_gpu_sg_relu_grad(_p(dA), _p(a), dA.numel(), _p(gn), None))
+                g = gn
+        return float(loss.item()), dW, db
+
+    def apply(self, dW, db, lr: float = 1e-3, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+        self.step_count += 1
+        L = _lib()
+        for l in range(len(self.W)):
+            api._check(L.solar_gpu_sg_adam(_p(self.W[l]), _p(dW[l]), _p(self.mW[l]), _p(self.vW[l]),
+                                           self.W[l].numel(), lr, b1, b2, eps, self.step_count, _p(self.Wb[l]),
+                                           None))
+            api._check(L.solar_gpu_sg_adam(_p(self.b[l]), _p(db[l]), _p(self.mb[l]), _p(self.vb[l]),
+                                           self.b[l].numel(), lr, b1, b2, eps, self.step_count, None, None))
+
+    def train(self, data: list, steps: int, batch: int = 1024, lr: float = 1e-3, seed: int = 0, log_every: int = 0):
+        """data: (scene, dev arrays, shadow words on the device, words32) per
+        training scene; batches of `batch` voxels drawn uniformly."""
+        torch = self.torch
+        rng = np.random.default_rng(seed)
+        losses = []
+        for it in range(steps):
+            scene, dev, shadow, words32 = data[it % len(data)]
+            vox = torch.from_numpy(rng.integers(0, scene.num_total, batch, dtype=np.int32)).to(self.dev)
+            X = self.features(scene, dev, vox)
+            Y = self.labels(shadow, words32, vox)
+            loss, dW, db = self.gradients(X, Y)
+            self.apply(dW, db, lr)
+            losses.append(loss)
+            if log_every and (it + 1) % log_every == 0:
+                print(f"step {it + 1}: loss {np.mean(losses[-log_every:]):.4f}", flush=True)
+        return losses
+
+    def predict_bits(self, scene, dev: dict, voxels, batch: int = 16384):
+        """Predicted shadow words [n][ceil(active/32)] (uint32, on the device)."""
+        torch = self.torch
+        n = voxels.numel()
+        words = (self.active + 31) // 32
+        out = torch.zeros(n, words, dtype=torch.int64, device=self.dev)
+        shifts = (torch.arange(32, device=self.dev, dtype=torch.int64))
+        for i0 in range(0, n, batch):
+            v = voxels[i0:i0 + batch]
+            m = v.numel()
+            pad = (-m) % 128
+            if pad:
+                v = torch.cat([v, v[:1].expand(pad)])
+            _, Z = self.forward(self.features(scene, dev, v))
+            bits = (Z[:m, :self.active] > 0).to(torch.int64)
+            bits = torch.nn.functional.pad(bits, (0, 32 * words - self.active))
+            out[i0:i0 + m] = (bits.view(m, words, 32) << shifts).sum(-1)
+        return out.to(torch.int32)   # low 32 bits carry the word
+
+
+def exact_bits(ctx, scene, dev: dict, voxels) -> tuple:
+    """Exact DDA shadow words of the listed voxels (device int32 ids)."""
+    import torch
+    n = voxels.numel()
+    words = C.c_int(0)
+    d, keep = api._scene_desc(scene, dev)
+    # first call sizes the words: trace zero voxels
+    api._check(_lib().solar_gpu_trace_shadow_subset(ctx.h, C.byref(d), _p(voxels), 0, _p(voxels), C.byref(words),
+                                                    None))
+    out = torch.zeros(max(1, n), words.value, dtype=torch.int32, device=voxels.device)
+    api._check(_lib().solar_gpu_trace_shadow_subset(ctx.h, C.byref(d), _p(voxels), n, _p(out), C.byref(words),
+                                                    None))
+    return out[:n], words.value
+
+
+def bit_error(pred, exact, active: int) -> float:
+    """Fraction of the active sun bins whose bit differs."""
+    import torch
+    x = (pred ^ exact).to(torch.int64) & 0xFFFFFFFF
+    diff = sum(int(((x >> k) & 1).sum()) for k in range(32))
+    return diff / (pred.shape[0] * active)
+
+
+def predict_with_fallback(model: Surrogate, ctx, scene, dev: dict, tile: int = 256, spot: int = 64,
+                          max_err: float = 0.02, seed: int = 0) -> dict:
+    """Shadow words of every voxel: the model's, checked per tile on `spot`
+    random voxels against the exact tracer; tiles above `max_err` traced
+    exactly.  Returns the words and per-tile statistics."""
+    import torch
+    t0 = time.perf_counter()
+    allv = torch.arange(scene.num_total, dtype=torch.int32, device=model.dev)
+    words = model.predict_bits(scene, dev, allv)
+    torch.cuda.synchronize()
+    t_model = time.perf_counter() - t0
+    pp = scene.pixel_parent.astype(np.int64)
+    tid = (pp % scene.width) // tile + ((pp // scene.width) // tile) * ((scene.width + tile - 1) // tile)
+    rng = np.random.default_rng(seed)
+    stats = []
+    for t in np.unique(tid):
+        members = np.nonzero(tid == t)[0].astype(np.int32)
+        smp = torch.from_numpy(rng.choice(members, min(spot, members.size), replace=False).astype(np.int32)).to(model.dev)
+        ex, _ = exact_bits(ctx, scene, dev, smp)
+        err = bit_error(words[smp.long()], ex, model.active)
+        fell_back = err > max_err
+        if fell_back:
+            mv = torch.from_numpy(members).to(model.dev)
+            exm, _ = exact_bits(ctx, scene, dev, mv)
+            words[mv.long()] = exm
+        stats.append({"tile": int(t), "voxels": int(members.size), "sampled_error": err, "fallback": bool(fell_back)})
+    torch.cuda.synchronize()
+    return {"words": words, "tiles": stats, "model_s": t_model, "total_s": time.perf_counter() - t0}

@@ -29,3 +29,76 @@ def test_gemm_rejects_bad_shapes():
     rc = api.lib().solar_gpu_gemm_bf16(C.c_void_p(16), C.c_void_p(32), C.c_void_p(64), None, None, 100, 128, 64, 0,
                                        None)
     assert rc in (-1, -2, -3)
+
+
+def _bf16(x):
+    """Round float values to bfloat16 (nearest even), returned as float64."""
+    import numpy as np
+    f = np.asarray(x, np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+@pytest.mark.gpu
+def test_surrogate_gradients_match_fp64():
+    """Backward pass (all products on the tensor cores) against an FP64 numpy
+    restatement that rounds to bf16 where the GPU path stores bf16."""
+    import numpy as np
+    import torch
+    from solargpu_b200 import surrogate as S
+    M, active = 128, 100
+    m = S.Surrogate(active=active, hidden=128, layers=1, feat=128, outw=128, seed=3)
+    g = torch.Generator(device="cpu").manual_seed(7)
+    X = torch.randn(M, 128, generator=g).to(torch.bfloat16).cuda()
+    Y = (torch.rand(M, 128, generator=g) > 0.5).float().cuda()
+    m.b[0].copy_(torch.randn(128, generator=g) * 0.1)
+    m.b[1].copy_(torch.randn(128, generator=g) * 0.1)
+    loss, dW, db = m.gradients(X, Y)
+    x = X.float().cpu().numpy().astype(np.float64)
+    y = Y.cpu().numpy().astype(np.float64)
+    w1, w2 = (w.float().cpu().numpy().astype(np.float64) for w in m.Wb)
+    b1, b2 = (b.cpu().numpy().astype(np.float64) for b in m.b)
+    h1 = _bf16(np.maximum(x @ w1.T + b1, 0.0))
+    z = h1 @ w2.T + b2
+    mask = np.arange(128) < active
+    p = 1.0 / (1.0 + np.exp(-z))
+    dz = _bf16(np.where(mask, (p - y) / (M * active), 0.0))
+    ref_loss = np.sum(np.where(mask, np.maximum(z, 0) - z * y + np.log1p(np.exp(-np.abs(z))), 0.0)) / (M * active)
+    g1 = _bf16(np.where(h1 > 0, dz @ w2, 0.0))
+    refs = [(g1.T @ x, g1.sum(0)), (dz.T @ h1, dz.sum(0))]
+    assert abs(loss - ref_loss) <= 1e-4 * abs(ref_loss)
+    for l, (rw, rb) in enumerate(refs):
+        gw = dW[l].cpu().numpy()
+        gb = db[l].cpu().numpy()
+        assert np.abs(gw - rw).max() <= 2e-2 * np.abs(rw).max(), l
+        assert np.abs(gb - rb).max() <= 2e-2 * np.abs(rb).max(), l
+        assert np.abs(gw - rw).mean() <= 2e-3 * np.abs(rw).mean(), l
+
+
+@pytest.mark.gpu
+def test_surrogate_learns_and_fallback_is_exact():
+    """A short training run lowers the loss; with a zero error threshold the
+    guarded prediction falls back everywhere and equals the exact DDA bits."""
+    import numpy as np
+    import torch
+    from conftest import device_arrays, load_scene
+    from solargpu_b200 import api
+    from solargpu_b200 import surrogate as S
+    s = load_scene("dsm64")
+    dev = device_arrays(s)
+    with api.Context(0) as ctx:
+        r = ctx.trace(s, dev, neighbor_format=0)
+        sh = torch.from_numpy(r["shadow"].view(np.int32)).cuda()
+        m = S.Surrogate(active=r["active_bins"], seed=1)
+        losses = m.train([(s, dev, sh, r["shadow_words"])], steps=60, batch=256, lr=1e-3)
+        assert np.mean(losses[-10:]) < np.mean(losses[:10])
+        res = S.predict_with_fallback(m, ctx, s, dev, tile=32, spot=16, max_err=0.0)
+        allv = torch.arange(s.num_total, dtype=torch.int32, device="cuda")
+        exact, w = S.exact_bits(ctx, s, dev, allv)
+        assert w == r["shadow_words"]
+        assert torch.equal(exact.cpu(), sh.cpu())
+        # every tile whose sample showed any error was replaced by exact bits
+        for t in res["tiles"]:
+            if t["sampled_error"] > 0:
+                assert t["fallback"]
