@@ -238,3 +238,86 @@ def predict_with_fallback(model: Surrogate, ctx, scene, dev: dict, tile: int = 2
         stats.append({"tile": int(t), "voxels": int(members.size), "sampled_error": err, "fallback": bool(fell_back)})
     torch.cuda.synchronize()
     return {"words": words, "tiles": stats, "model_s": t_model, "total_s": time.perf_counter() - t0}
+
+
+def main(argv=None) -> int:
+    """Train on some synthetic cities, then the guarded prediction on another
+    against the exact tracer (the ablation):
+
+        python -m solargpu_b200.surrogate [--train dsm256,dsm512] [--test dsm1024] [--steps 3000]
+    """
+    import argparse
+    import json
+    import torch
+    from . import inputs
+    ap = argparse.ArgumentParser(description="sky-bin visibility surrogate: train and ablation")
+    ap.add_argument("--train", default="dsm256,dsm512")
+    ap.add_argument("--test", default="dsm1024")
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=1024)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--max-err", type=float, default=0.02)
+    a = ap.parse_args(argv)
+
+    def staged(name):
+        s = inputs.make_scene(name)
+        d = {"grid": torch.from_numpy(s.grid).cuda(), "pixel_parent": torch.from_numpy(s.pixel_parent).cuda(),
+             "wall_z": torch.from_numpy(s.wall_z if s.wall_z.size else np.zeros(1, np.float32)).cuda(),
+             "slopes": torch.from_numpy(s.slopes).cuda(), "aspects": torch.from_numpy(s.aspects).cuda()}
+        return s, d
+
+    res = {}
+    with api.Context(0) as ctx:
+        data = []
+        for name in a.train.split(","):
+            s, d = staged(name)
+            r = ctx.trace(s, d, neighbor_format=0)
+            data.append((s, d, torch.from_numpy(r["shadow"].view(np.int32)).cuda(), r["shadow_words"]))
+            active = r["active_bins"]
+        model = Surrogate(active=active, seed=0)
+        t0 = time.perf_counter()
+        losses = model.train(data, a.steps, a.batch, a.lr)
+        torch.cuda.synchronize()
+        res["train"] = {"scenes": a.train, "steps": a.steps, "batch": a.batch, "s": round(time.perf_counter() - t0, 2),
+                        "loss_first100": float(np.mean(losses[:100])), "loss_last100": float(np.mean(losses[-100:]))}
+        s, d = staged(a.test)
+        allv = torch.arange(s.num_total, dtype=torch.int32, device="cuda")
+        # exact shadow words of every voxel (chunks of 2^20), timed
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        exact = torch.cat([exact_bits(ctx, s, d, allv[i:i + (1 << 20)])[0] for i in range(0, s.num_total, 1 << 20)])
+        torch.cuda.synchronize()
+        t_exact = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        pred = model.predict_bits(s, d, allv)
+        torch.cuda.synchronize()
+        t_pred = time.perf_counter() - t0
+        guarded = predict_with_fallback(model, ctx, s, d, max_err=a.max_err)
+        res["test"] = {"scene": a.test, "voxels": s.num_total, "active_bins": active,
+                       "exact_trace_s": round(t_exact, 4), "model_only_s": round(t_pred, 4),
+                       "model_bit_error": bit_error(pred, exact, active),
+                       "guarded_s": round(guarded["total_s"], 4),
+                       "guarded_bit_error": bit_error(guarded["words"], exact, active),
+                       "tiles": len(guarded["tiles"]),
+                       "fallback_tiles": sum(t["fallback"] for t in guarded["tiles"])}
+        # tensor-core GEMM throughput on one large product (the surrogate's kernel)
+        Mg, Ng, Kg = 8192, 8192, 4096
+        A = torch.randn(Mg, Kg, device="cuda").to(torch.bfloat16)
+        B = torch.randn(Ng, Kg, device="cuda").to(torch.bfloat16)
+        Cg = torch.empty(Mg, Ng, device="cuda")
+        api.gemm_bf16(A, B, out=Cg)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            api.gemm_bf16(A, B, out=Cg)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        res["gemm"] = {"M": Mg, "N": Ng, "K": Kg, "ms": round(ms, 3), "tflops": round(2.0 * Mg * Ng * Kg / ms / 1e9, 1)}
+    print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())
