@@ -257,7 +257,11 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--max-err", type=float, default=0.02)
+    ap.add_argument("--gemm-only", type=int, default=0, metavar="SIZE",
+                    help="only time the tensor-core GEMM on SIZE x SIZE x SIZE (profiling)")
     a = ap.parse_args(argv)
+    if a.gemm_only:
+        return _gemm_bench(a.gemm_only, a.gemm_only, a.gemm_only)
 
     def staged(name):
         s = inputs.make_scene(name)
@@ -300,21 +304,31 @@ def main(argv=None) -> int:
                        "guarded_bit_error": bit_error(guarded["words"], exact, active),
                        "tiles": len(guarded["tiles"]),
                        "fallback_tiles": sum(t["fallback"] for t in guarded["tiles"])}
-        # tensor-core GEMM throughput on one large product (the surrogate's kernel)
-        Mg, Ng, Kg = 8192, 8192, 4096
-        A = torch.randn(Mg, Kg, device="cuda").to(torch.bfloat16)
-        B = torch.randn(Ng, Kg, device="cuda").to(torch.bfloat16)
-        Cg = torch.empty(Mg, Ng, device="cuda")
-        api.gemm_bf16(A, B, out=Cg)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(5):
-            api.gemm_bf16(A, B, out=Cg)
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1) / 5
-        res["gemm"] = {"M": Mg, "N": Ng, "K": Kg, "ms": round(ms, 3), "tflops": round(2.0 * Mg * Ng * Kg / ms / 1e9, 1)}
+        res["gemm"] = _gemm_stats(8192, 8192, 4096)
     print(json.dumps(res))
+    return 0
+
+
+def _gemm_stats(Mg: int, Ng: int, Kg: int, reps: int = 5) -> dict:
+    """Time of C = A B^T on the tensor cores (CUDA events, after one warm run)."""
+    import torch
+    A = torch.randn(Mg, Kg, device="cuda").to(torch.bfloat16)
+    B = torch.randn(Ng, Kg, device="cuda").to(torch.bfloat16)
+    Cg = torch.empty(Mg, Ng, device="cuda")
+    api.gemm_bf16(A, B, out=Cg)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        api.gemm_bf16(A, B, out=Cg)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return {"M": Mg, "N": Ng, "K": Kg, "ms": round(ms, 3), "tflops": round(2.0 * Mg * Ng * Kg / ms / 1e9, 1)}
+
+
+def _gemm_bench(Mg: int, Ng: int, Kg: int) -> int:
+    import json
+    print(json.dumps({"gemm": _gemm_stats(Mg, Ng, Kg, reps=3)}))
     return 0
 
 
