@@ -2,39 +2,51 @@
 // visibility surrogate:   C[M][N] (f32) = A[M][K] (bf16) x B[N][K]^T (bf16)
 // (+ bias[N], optional ReLU, optional bf16 copy of the result).
 //
-// One CTA of 128 threads per 128 x 128 output tile.  Per K step of 64:
-//   * the 4 warps copy the A and B tiles (128 x 64 bf16 each) from global
-//     memory into shared memory in the canonical K-major layout without
-//     swizzle: core matrices of 8 rows x 16 bytes (8 bf16), core matrix
-//     (row group g, K block b) at byte (b * 16 + g) * 128, so the leading
-//     (K-direction) byte offset is 2048 and the stride (row-direction) one
-//     is 128;
-//   * a proxy fence makes the generic-proxy stores visible to the tensor
-//     core, and one elected thread issues 4 tcgen05.mma (K = 16 each,
-//     M = 128, N = 128, f32 accumulator in 128 TMEM columns), then
-//     tcgen05.commit arrives on an mbarrier that all threads wait on
-//     (bounded by the global timer, like every wait in this library).
-// Epilogue: each warp reads its 32 TMEM lanes (rows) with tcgen05.ld
-// 32x32b.x8, adds the bias, applies ReLU and stores rows of C.
-// The TMEM columns are allocated by warp 0 at the start and freed at the end.
+// One CTA of 128 threads per 128 x BN output tile (BN = 256 when N allows,
+// else 128), K in steps of 64 through a ring of kGemmStages shared-memory
+// stages:
+//   * thread 0 (producer) loads each stage with tensor-map TMA, one box of
+//     64 bf16 (128 bytes) x rows per operand, 128-byte swizzle: this is the
+//     canonical K-major SWIZZLE_128B layout the tensor core reads (8-row
+//     atoms of 1024 bytes, 16-byte chunks XOR-ed with the row within the
+//     atom); completion is counted in bytes on the stage's full mbarrier;
+//   * thread 32 (MMA issuer) waits for a stage, issues 4 tcgen05.mma (K = 16
+//     each, 32 bytes further along the swizzled rows; M = 128, N = BN, f32
+//     accumulator in BN TMEM columns) and tcgen05.commit frees the stage
+//     (empty mbarrier) when they complete; a last commit signals the
+//     epilogue;
+//   * epilogue: each warp reads its 32 TMEM lanes (rows) with tcgen05.ld
+//     32x32b.x8, adds the bias, applies ReLU and stores rows of C.
+// Every wait is bounded by the global timer; on expiry the kernel flags the
+// error, lets its TMA copies and MMAs finish (bounded), frees TMEM and exits.
 // M and N must be multiples of 128, K a multiple of 64 (the caller pads).
 #include "sgb_internal.cuh"
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 namespace sgb {
 namespace {
 
-constexpr int kTm = 128, kTn = 128, kTk = 64;
+constexpr int kTm = 128, kTk = 64;
 constexpr int kGemmThreads = 128;
-// Each CTA holds 128 TMEM columns; 14 KB of (unused) dynamic shared memory on
-// top of the 33 KB of tiles keeps at most 4 CTAs on an SM, so the 512
-// columns always suffice and tcgen05.alloc never waits.
-constexpr int kGemmSmemPad = 14 * 1024;
+constexpr int kGemmStages = 4;
 constexpr unsigned long long kGemmWaitNs = 1000000000ull;   // 1 s
+
+template <int BN>
+struct GemmShape {
+    static constexpr int kStageA = kTm * kTk * 2, kStageB = BN * kTk * 2;     // 16 KB, 16/32 KB
+    static constexpr int kStage = kStageA + kStageB;
+    static constexpr int kSmem = kGemmStages * kStage + 1024;              // + alignment slack
+    // Instruction descriptor, kind::f16: f32 accumulator, bf16 A and B,
+    // both K-major, N = BN, M = 128.
+    static constexpr unsigned kIdesc =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(BN >> 3) << 17) | ((unsigned)(kTm >> 4) << 24);
+};
 
 __device__ __forceinline__ unsigned s_u32(const void* p)
 {
@@ -48,7 +60,7 @@ __device__ __forceinline__ unsigned long long g_ns()
     return t;
 }
 
-__device__ __forceinline__ bool wait_parity(unsigned bar, unsigned parity)
+__device__ __forceinline__ bool wait_parity(unsigned bar, unsigned parity, const volatile int* fail)
 {
     unsigned long long t0 = 0;
     for (unsigned i = 0;; ++i) {
@@ -62,6 +74,7 @@ __device__ __forceinline__ bool wait_parity(unsigned bar, unsigned parity)
             : "memory");
         if (ok) return true;
         if ((i & 63u) == 63u) {
+            if (fail && *fail) return false;
             const unsigned long long t = g_ns();
             if (t0 == 0) t0 = t;
             else if (t - t0 > kGemmWaitNs) return false;
@@ -69,52 +82,50 @@ __device__ __forceinline__ bool wait_parity(unsigned bar, unsigned parity)
     }
 }
 
-// Shared-memory matrix descriptor, K-major, no swizzle (version 1 = sm_100).
-__device__ __forceinline__ unsigned long long smem_desc(unsigned addr, unsigned lbo, unsigned sbo)
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle (layout type 2,
+// version 1 = sm_100): stride between 8-row atoms 1024 bytes, leading offset
+// unused (16 bytes), atoms 1024-byte aligned so the base offset is 0.
+__device__ __forceinline__ unsigned long long smem_desc_sw128(unsigned addr)
 {
-    return (unsigned long long)((addr >> 4) & 0x3FFFu) | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+    return (unsigned long long)((addr >> 4) & 0x3FFFu) | (1ull << 16) | ((unsigned long long)(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
 }
 
-// Instruction descriptor, kind::f16: f32 accumulator, bf16 A and B, both
-// K-major, N = 128, M = 128.
-constexpr unsigned kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(kTn >> 3) << 17) |
-                            ((unsigned)(kTm >> 4) << 24);
-
-// Copies a 128 x 64 bf16 tile (rows r0.., columns k0..) of a row-major
-// matrix with `ld` elements per row into the canonical layout.
-__device__ __forceinline__ void load_tile(unsigned char* dst, const __nv_bfloat16* __restrict__ src, int ld,
-                                          int r0, int k0)
+__device__ __forceinline__ void tma_box(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar)
 {
-#pragma unroll
-    for (int i = 0; i < (kTm * kTk / 8) / kGemmThreads; ++i) {
-        const int c = threadIdx.x + kGemmThreads * i;   // 16-byte chunk: row c / 8, K block c % 8
-        const int row = c >> 3, kb = c & 7;
-        const uint4 v = *reinterpret_cast<const uint4*>(src + (size_t)(r0 + row) * ld + k0 + 8 * kb);
-        *reinterpret_cast<uint4*>(dst + (kb * (kTm / 8) + (row >> 3)) * 128 + (row & 7) * 16) = v;
-    }
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+                 : "memory");
 }
 
-__global__ void __launch_bounds__(kGemmThreads)
-k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B, float* __restrict__ C,
-            __nv_bfloat16* __restrict__ Cb, const float* __restrict__ bias, int M, int N, int K, int relu,
-            int* __restrict__ err)
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads, 1)
+k_gemm_bf16(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+            float* __restrict__ C, __nv_bfloat16* __restrict__ Cb, const float* __restrict__ bias, int M, int N, int K,
+            int relu, int* __restrict__ err)
 {
-    __shared__ __align__(128) unsigned char sa[kTm * kTk * 2];
-    __shared__ __align__(128) unsigned char sb[kTn * kTk * 2];
-    __shared__ __align__(8) unsigned long long mma_bar;
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    __shared__ __align__(8) unsigned long long full[kGemmStages], empty[kGemmStages], done;
     __shared__ unsigned tmem_base;
-    __shared__ int s_fail;
+    __shared__ volatile int s_fail;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * kTm, n0 = blockIdx.x * kTn;
+    using S = GemmShape<BN>;
+    const int m0 = blockIdx.y * kTm, n0 = blockIdx.x * BN;
+    // 1024-byte aligned stage ring
+    const unsigned base = (s_u32(gsm) + 1023u) & ~1023u;
+    const int nk = K / kTk;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_u32(&tmem_base)),
-                     "r"(kTn));
+                     "r"(BN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&mma_bar)), "r"(1));
+        for (int s = 0; s < kGemmStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&full[s])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&empty[s])), "r"(1));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&done)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
     }
@@ -123,44 +134,65 @@ k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned tmem = tmem_base;
 
-    const unsigned a0 = s_u32(sa), b0 = s_u32(sb);
-    constexpr unsigned kLbo = (kTm / 8) * 128, kSbo = 128;
-    unsigned phase = 0;
-    for (int k0 = 0; k0 < K; k0 += kTk) {
-        load_tile(sa, A, K, m0, k0);
-        load_tile(sb, B, K, n0, k0);
-        // generic-proxy shared stores -> visible to the tensor core's async proxy
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0) {
+    int issued = 0;   // producer: stages loaded
+    if (threadIdx.x == 0) {
+        // ---- producer
+        for (int k = 0; k < nk; ++k) {
+            const int s = k % kGemmStages;
+            if (k >= kGemmStages &&
+                !wait_parity(s_u32(&empty[s]), (unsigned)(((k / kGemmStages) - 1) & 1), &s_fail)) {
+                s_fail = 1;
+                break;
+            }
+            const unsigned sa = base + (unsigned)(s * S::kStage), sb = sa + S::kStageA;
+            const unsigned fb = s_u32(&full[s]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                         "r"((unsigned)S::kStage) : "memory");
+            tma_box(sa, &mapA, k * kTk, m0, fb);
+            tma_box(sb, &mapB, k * kTk, n0, fb);
+            ++issued;
+        }
+    } else if (threadIdx.x == 32) {
+        // ---- MMA issuer
+        int k = 0;
+        for (; k < nk; ++k) {
+            const int s = k % kGemmStages;
+            if (!wait_parity(s_u32(&full[s]), (unsigned)((k / kGemmStages) & 1), &s_fail)) {
+                s_fail = 1;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned sa = base + (unsigned)(s * S::kStage), sb = sa + S::kStageA;
 #pragma unroll
-            for (int s = 0; s < kTk / 16; ++s) {
-                const unsigned long long da = smem_desc(a0 + 2 * s * kLbo, kLbo, kSbo);
-                const unsigned long long db = smem_desc(b0 + 2 * s * kLbo, kLbo, kSbo);
-                const unsigned acc = (k0 > 0 || s > 0) ? 1u : 0u;
+            for (int j = 0; j < kTk / 16; ++j) {
+                const unsigned long long da = smem_desc_sw128(sa + 32u * j);
+                const unsigned long long db = smem_desc_sw128(sb + 32u * j);
+                const unsigned acc = (k > 0 || j > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                    ::"r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(S::kIdesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
             }
+            // the stage is free once these MMAs have read it
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         ::"r"(s_u32(&mma_bar)) : "memory");
+                         ::"r"(s_u32(&empty[s])) : "memory");
         }
-        // the MMAs read shared memory: wait for them before the next copy
-        if (!wait_parity(s_u32(&mma_bar), phase)) s_fail = 1;   // bounded
-        phase ^= 1u;
-        __syncthreads();
-        if (s_fail) break;
+        // all MMAs issued so far complete -> epilogue
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(s_u32(&done)) : "memory");
     }
+    // everyone: the accumulator is ready (or the run failed)
+    if (!wait_parity(s_u32(&done), 0u, nullptr)) s_fail = 1;
+    __syncthreads();
+    const bool ok = !s_fail;   // uniform over the CTA
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-    if (!s_fail) {
+    if (ok) {
         // epilogue: warp w holds rows 32w.. of the tile (TMEM lanes 32w..)
         const int row = m0 + 32 * warp + lane;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kTn; c0 += 8) {
+        for (int c0 = 0; c0 < BN; c0 += 8) {
             unsigned r[8];
             const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)c0;
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -188,12 +220,14 @@ k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict
         }
     } else if (threadIdx.x == 0) {
         atomicOr(err, kErrWaitTimeout);
-        wait_parity(s_u32(&mma_bar), phase ^ 1u);   // once more (bounded) before the TMEM is freed
+        // let the TMA copies this thread issued land before the CTA exits
+        for (int k = (issued > kGemmStages ? issued - kGemmStages : 0); k < issued; ++k)
+            wait_parity(s_u32(&full[k % kGemmStages]), (unsigned)((k / kGemmStages) & 1), nullptr);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTn));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
 }
 
 // ---- surrogate training and inference kernels ------------------------------
@@ -317,15 +351,74 @@ __global__ void k_sg_adam(float* __restrict__ p, const float* __restrict__ g, fl
 
 }  // namespace
 
+namespace {
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn()
+{
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+
+// Row-major [rows][K] bf16 matrix, boxes of 64 elements (128 bytes) x box_rows
+// rows with 128-byte swizzle.
+bool make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows)
+{
+    EncodeTiled fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)kTk, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN>
+cudaError_t launch_gemm_tiles(const void* A, const void* B, float* C, void* Cb, const float* bias, int M, int N,
+                              int K, int relu, int* err, cudaStream_t st)
+{
+    CUtensorMap mapA, mapB;
+    if (!make_map(&mapA, A, M, K, kTm) || !make_map(&mapB, B, N, K, BN)) return cudaErrorInvalidValue;
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+        e = cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmShape<BN>::kSmem);
+        if (e != cudaSuccess) return e;
+        attr[dev] = true;
+    }
+    const dim3 grid(N / BN, M / kTm);
+    k_gemm_bf16<BN><<<grid, kGemmThreads, GemmShape<BN>::kSmem, st>>>(
+        mapA, mapB, C, static_cast<__nv_bfloat16*>(Cb), bias, M, N, K, relu, err);
+    return cudaGetLastError();
+}
+}  // namespace
+
+// Tile width: 256 columns when N allows it and the grid still covers the
+// SMs (148 on B200) at least once, else 128.
 cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, const float* bias, int M, int N,
                              int K, int relu, int* err, cudaStream_t st)
 {
-    if (M <= 0 || N <= 0 || K <= 0 || M % kTm || N % kTn || K % kTk) return cudaErrorInvalidValue;
-    const dim3 grid(N / kTn, M / kTm);
-    k_gemm_bf16<<<grid, kGemmThreads, kGemmSmemPad, st>>>(static_cast<const __nv_bfloat16*>(A),
-                                                static_cast<const __nv_bfloat16*>(B), C,
-                                                static_cast<__nv_bfloat16*>(Cb), bias, M, N, K, relu, err);
-    return cudaGetLastError();
+    if (M <= 0 || N <= 0 || K <= 0 || M % kTm || N % 128 || K % kTk) return cudaErrorInvalidValue;
+    const char* force = getenv("SGB_GEMM_BN");
+    int bn = (N % 256 == 0 && (long long)(M / kTm) * (N / 256) >= 148) ? 256 : 128;
+    if (force && atoi(force) == 128) bn = 128;
+    if (force && atoi(force) == 256 && N % 256 == 0) bn = 256;
+    return bn == 256 ? launch_gemm_tiles<256>(A, B, C, Cb, bias, M, N, K, relu, err, st)
+                     : launch_gemm_tiles<128>(A, B, C, Cb, bias, M, N, K, relu, err, st);
 }
 
 }  // namespace sgb

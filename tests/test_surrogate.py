@@ -4,8 +4,11 @@ import pytest
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 320), (384, 256, 1024)])
-def test_gemm_bf16_matches_fp32_product(M, N, K):
+@pytest.mark.parametrize("bn", ["128", "256"])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 320), (384, 256, 1024), (256, 512, 1600)])
+def test_gemm_bf16_matches_fp32_product(M, N, K, bn, monkeypatch):
+    """Both tile widths (SGB_GEMM_BN forces one where N allows it)."""
+    monkeypatch.setenv("SGB_GEMM_BN", bn)
     import torch
     from solargpu_b200 import api
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
