@@ -234,8 +234,8 @@ int solar_gpu_trace_shadow_subset(solar_gpu_context* ctx, const solar_gpu_scene*
 /* No counterpart in the reference.  C[M][N] = A[M][K] x B[N][K]^T (+ bias[N],
    ReLU if relu != 0) on the tcgen05 tensor cores: A, B bf16 row-major (K
    contiguous), f32 accumulation in TMEM, output f32 (C) and/or bf16 (C_bf16),
-   row-major; device pointers, 16-byte aligned.  M and N multiples of 128, K a
-   multiple of 64.  Synchronous on `stream`. */
+   row-major; device pointers, 16-byte aligned.  M a multiple of 128, N of 64,
+   K of 64.  Synchronous on `stream`. */
 int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N,
                         int K, int relu, void* stream);
 
@@ -246,7 +246,8 @@ int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, co
    bits of each voxel as 0/1 floats over outw columns.  bce: mean binary
    cross-entropy with logits over the first `active` columns (adds to *loss),
    dZ = (sigmoid(Z) - Y) / (M active) as bf16.  relu_grad: dX = dY (H > 0).
-   transpose: out[C][R] = in[R][C].  colsum: out[c] = sum_r in[r][c].  adam:
+   transpose: out[C][R] = in[R][C].  colsum: out[c] = sum_r in[r][c] (out
+   overwritten).  adam:
    one Adam step on FP32 parameters (bias-corrected, step >= 1), optional
    bf16 copy. */
 int solar_gpu_sg_features(const float* grid, int W, int H, int T, const int* pixel_parent, const float* wall_z,
@@ -261,6 +262,30 @@ int solar_gpu_sg_transpose(const void* in_bf16, int R, int C, void* out_bf16, vo
 int solar_gpu_sg_colsum(const void* in_bf16, int R, int C, float* out, void* stream);
 int solar_gpu_sg_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
                       float eps, int step, void* p_bf16, void* stream);
+
+/* Convolutional front end of the surrogate (4 x 4 kernels, stride 2,
+   padding 1, NHWC bf16 activations).  coarse: out[cy][cx] = max of grid over
+   the 8 x 8 cells of context cell (cx, cy), ceil(H/8) x ceil(W/8).  image:
+   per voxel a [64][64][2] image, channel 0 the heights of the 64 x 64 cells
+   around its pixel, channel 1 the context maxima of the 64 x 64 context cells
+   around its context cell, both relative to its base height / 50 m (clipped
+   to +-2), and nrm [M][64] its normal zero-padded.  im2col: cols[(b Ho + oy)
+   Wo + ox][(ky 4 + kx) Cin + c] = X[b][2oy-1+ky][2ox-1+kx][c] (0 outside),
+   zero columns up to Kp.  col2im_relu: the gradient of X through im2col,
+   times (X > 0), as bf16.  hcat: rows of a and b side by side.
+   relu_grad_cols: out[r][c] = dY[r][c] (H[r][c] > 0) for c < cols, strided
+   inputs.  transpose_f32: out[C][R] = in[R][C]. */
+int solar_gpu_sg_coarse(const float* grid, int W, int H, float* out, void* stream);
+int solar_gpu_sg_image(const float* grid, const float* coarse, int W, int H, int T, const int* pixel_parent,
+                       const float* wall_z, const float* slopes, const float* aspects, const int* voxels, int M,
+                       void* img_bf16, void* nrm_bf16, void* stream);
+int solar_gpu_sg_im2col(const void* X_bf16, int B, int Hi, int Wi, int Cin, int Kp, void* cols_bf16, void* stream);
+int solar_gpu_sg_col2im_relu(const float* dcols, const void* X_bf16, int B, int Hi, int Wi, int Cin, int Kp,
+                             void* g_bf16, void* stream);
+int solar_gpu_sg_hcat(const void* a_bf16, int wa, const void* b_bf16, int wb, int rows, void* out_bf16, void* stream);
+int solar_gpu_sg_relu_grad_cols(const float* dY, int ldy, const void* H_bf16, int ldh, int rows, int cols,
+                                void* out_bf16, void* stream);
+int solar_gpu_sg_transpose_f32(const float* in, int R, int C, float* out, void* stream);
 
 /* ---- encoding without device allocation -------------------------------- */
 

@@ -175,7 +175,7 @@ def compressed_gpu_irradiance(grid_data, grid_width, grid_height, num_total_voxe
 
 def gemm_bf16(A, B, out=None, out_bf16=None, bias=None, relu: bool = False, stream=None):
     """C = A @ B.T (+ bias, ReLU) on the tensor cores; A [M, K], B [N, K]
-    bf16 CUDA tensors (contiguous), M and N multiples of 128, K of 64."""
+    bf16 CUDA tensors (contiguous), M a multiple of 128, N and K of 64."""
     import torch
     M, K = A.shape
     N = B.shape[0]

@@ -3,7 +3,7 @@
 // (+ bias[N], optional ReLU, optional bf16 copy of the result).
 //
 // One CTA of 128 threads per 128 x BN output tile (BN = 256 when N allows,
-// else 128), K in steps of 64 through a ring of kGemmStages shared-memory
+// 64 for 64-wide outputs, else 128), K in steps of 64 through a ring of kGemmStages shared-memory
 // stages:
 //   * thread 0 (producer) loads each stage with tensor-map TMA, one box of
 //     64 bf16 (128 bytes) x rows per operand, 128-byte swizzle: this is the
@@ -310,7 +310,7 @@ __global__ void k_sg_relu_grad(const float* __restrict__ dY, const __nv_bfloat16
 __global__ void k_sg_transpose(const __nv_bfloat16* __restrict__ in, int R, int C, __nv_bfloat16* __restrict__ out)
 {
     __shared__ __nv_bfloat16 t[32][33];
-    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;   // row tiles on x (up to 2^31 - 1)
     for (int k = threadIdx.y; k < 32; k += blockDim.y) {
         const int r = r0 + k, c = c0 + threadIdx.x;
         if (r < R && c < C) t[k][threadIdx.x] = in[(size_t)r * C + c];
@@ -322,14 +322,17 @@ __global__ void k_sg_transpose(const __nv_bfloat16* __restrict__ in, int R, int 
     }
 }
 
-// out[c] = sum over rows of in[r][c] (bias gradients).
-__global__ void k_sg_colsum(const __nv_bfloat16* __restrict__ in, int R, int C, float* __restrict__ out)
+// out[c] += sum over the rows r0 .. r0 + rows_per_block of in[r][c] (bias
+// gradients; out zeroed first, one atomic add per column and block).
+__global__ void k_sg_colsum(const __nv_bfloat16* __restrict__ in, int R, int C, int rows_per_block,
+                            float* __restrict__ out)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= C) return;
+    const int r0 = blockIdx.y * rows_per_block, r1 = min(R, r0 + rows_per_block);
     float s = 0.0f;
-    for (int r = 0; r < R; ++r) s += __bfloat162float(in[(size_t)r * C + c]);
-    out[c] = s;
+    for (int r = r0; r < r1; ++r) s += __bfloat162float(in[(size_t)r * C + c]);
+    atomicAdd(out + c, s);
 }
 
 // Adam on FP32 master parameters; the bf16 copy feeds the GEMMs.
@@ -346,6 +349,181 @@ __global__ void k_sg_adam(float* __restrict__ p, const float* __restrict__ g, fl
         const float q = p[t] - lr * (mt / c1) / (sqrtf(vt / c2) + eps);
         p[t] = q;
         if (pb) pb[t] = __float2bfloat16_rn(q);
+    }
+}
+
+// ---- convolutional front end (4 x 4 kernels, stride 2, padding 1, NHWC) ----
+
+constexpr int kCoarse = 8;   // cells per side of one context (max-pooled) cell
+
+// out[cy][cx] = max of grid over the kCoarse x kCoarse cells of (cx, cy).
+__global__ void k_sg_coarse(const float* __restrict__ grid, int W, int H, int Wc, int Hc, float* __restrict__ out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Wc * Hc) return;
+    const int cx = c % Wc, cy = c / Wc;
+    float m = -3.0e38f;
+    for (int y = cy * kCoarse; y < min(H, (cy + 1) * kCoarse); ++y)
+        for (int x = cx * kCoarse; x < min(W, (cx + 1) * kCoarse); ++x) m = fmaxf(m, grid[y * W + x]);
+    out[c] = m;
+}
+
+// Two-channel image of voxel voxels[i], NHWC [64][64][2]: channel 0 the
+// heights of the 64 x 64 cells around its pixel, channel 1 the maxima of the
+// 64 x 64 context cells (kCoarse x kCoarse cells each) around its context
+// cell, both relative to the voxel's base height, / 50 m, clipped to [-2, 2]
+// (outside the grid: 0 m).  nrm[i] = the voxel normal, zero-padded to 64.
+__global__ void k_sg_image(const float* __restrict__ grid, const float* __restrict__ coarse, int W, int H, int T,
+                           const int* __restrict__ pp, const float* __restrict__ wall_z,
+                           const float* __restrict__ slopes, const float* __restrict__ aspects,
+                           const int* __restrict__ voxels, int M, __nv_bfloat162* __restrict__ img,
+                           __nv_bfloat16* __restrict__ nrm)
+{
+    const int i = blockIdx.y;
+    if (i >= M) return;
+    const int v = voxels[i];
+    const int top = pp[v];
+    const int gx = top % W, gy = top / W;
+    const float z = v < T ? grid[top] : wall_z[v - T];
+    const int Wc = (W + kCoarse - 1) / kCoarse, Hc = (H + kCoarse - 1) / kCoarse;
+    const int cgx = gx / kCoarse, cgy = gy / kCoarse;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < kPatch * kPatch; j += gridDim.x * blockDim.x) {
+        const int dx = (j % kPatch) - kPatch / 2, dy = (j / kPatch) - kPatch / 2;
+        const int x = gx + dx, y = gy + dy, cx = cgx + dx, cy = cgy + dy;
+        const float h = (x >= 0 && x < W && y >= 0 && y < H) ? grid[y * W + x] : 0.0f;
+        const float hc = (cx >= 0 && cx < Wc && cy >= 0 && cy < Hc) ? coarse[cy * Wc + cx] : 0.0f;
+        img[(size_t)i * kPatch * kPatch + j] = __floats2bfloat162_rn(fminf(2.0f, fmaxf(-2.0f, (h - z) * kPatchScale)),
+                                                                     fminf(2.0f, fmaxf(-2.0f, (hc - z) * kPatchScale)));
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 64) {
+        const int c = threadIdx.x;
+        float f = 0.0f;
+        if (c < 3) {
+            const float sl = slopes[v] * 0.017453292f, as = aspects[v] * 0.017453292f;
+            f = c == 0 ? sinf(sl) * sinf(as) : c == 1 ? -sinf(sl) * cosf(as) : cosf(sl);
+        }
+        nrm[(size_t)i * 64 + c] = __float2bfloat16_rn(f);
+    }
+}
+
+// im2col for a 4 x 4, stride-2, padding-1 convolution over X [B][Hi][Wi][Cin]:
+// cols[(b * Ho + oy) * Wo + ox][(ky * 4 + kx) * Cin + c] = X[b][2oy-1+ky][2ox-1+kx][c]
+// (0 outside the image), columns 16 * Cin .. Kp - 1 zero.  One thread per 8
+// consecutive columns (Cin % 8 == 0: one 16-byte load and store).
+__global__ void k_sg_im2col(const __nv_bfloat16* __restrict__ X, int B, int Hi, int Wi, int Cin, int Kp,
+                            __nv_bfloat16* __restrict__ cols)
+{
+    const int Ho = Hi / 2, Wo = Wi / 2, K = 16 * Cin, g8 = Kp / 8;
+    const long long n = (long long)B * Ho * Wo * g8;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long row = t / g8;
+        const int k0 = (int)(t % g8) * 8;
+        const int ox = (int)(row % Wo), oy = (int)((row / Wo) % Ho);
+        const long long b = row / ((long long)Wo * Ho);
+        uint4 out = make_uint4(0u, 0u, 0u, 0u);
+        if (Cin % 8 == 0) {
+            if (k0 < K) {
+                const int tap = k0 / Cin, c = k0 % Cin;
+                const int y = 2 * oy - 1 + tap / 4, x = 2 * ox - 1 + tap % 4;
+                if (y >= 0 && y < Hi && x >= 0 && x < Wi)
+                    out = *reinterpret_cast<const uint4*>(X + (((size_t)b * Hi + y) * Wi + x) * Cin + c);
+            }
+        } else {
+            __nv_bfloat16 e[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = k0 + q;
+                e[q] = __float2bfloat16_rn(0.0f);
+                if (k < K) {
+                    const int tap = k / Cin, c = k % Cin;
+                    const int y = 2 * oy - 1 + tap / 4, x = 2 * ox - 1 + tap % 4;
+                    if (y >= 0 && y < Hi && x >= 0 && x < Wi) e[q] = X[(((size_t)b * Hi + y) * Wi + x) * Cin + c];
+                }
+            }
+            out = *reinterpret_cast<uint4*>(e);
+        }
+        *reinterpret_cast<uint4*>(cols + row * Kp + k0) = out;
+    }
+}
+
+// Backward of k_sg_im2col fused with the ReLU of the layer below:
+// g[b][y][x][c] = bf16( (X[b][y][x][c] > 0) * sum over the (<= 2 x 2) output
+// positions whose 4 x 4 window covers (y, x) of dcols[row][tap * Cin + c] ).
+// One thread per 8 channels (Cin % 8 == 0).
+__global__ void k_sg_col2im_relu(const float* __restrict__ dcols, const __nv_bfloat16* __restrict__ X, int B, int Hi,
+                                 int Wi, int Cin, int Kp, __nv_bfloat16* __restrict__ g)
+{
+    const int Ho = Hi / 2, Wo = Wi / 2, g8 = Cin / 8;
+    const long long n = (long long)B * Hi * Wi * g8;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long pix = t / g8;
+        const int c0 = (int)(t % g8) * 8;
+        const int x = (int)(pix % Wi), y = (int)((pix / Wi) % Hi);
+        const long long b = pix / ((long long)Wi * Hi);
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const int oy = ((y + 1) >> 1) - a, ky = y + 1 - 2 * oy;
+            if (oy < 0 || oy >= Ho) continue;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int ox = ((x + 1) >> 1) - e, kx = x + 1 - 2 * ox;
+                if (ox < 0 || ox >= Wo) continue;
+                const float4* src = reinterpret_cast<const float4*>(
+                    dcols + (((size_t)b * Ho + oy) * Wo + ox) * Kp + (ky * 4 + kx) * Cin + c0);
+                const float4 u = src[0], w = src[1];
+                acc[0] += u.x; acc[1] += u.y; acc[2] += u.z; acc[3] += u.w;
+                acc[4] += w.x; acc[5] += w.y; acc[6] += w.z; acc[7] += w.w;
+            }
+        }
+        const uint4 xv = *reinterpret_cast<const uint4*>(X + (size_t)pix * Cin + c0);
+        const __nv_bfloat16* xe = reinterpret_cast<const __nv_bfloat16*>(&xv);
+        __nv_bfloat16 o[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) o[q] = __float2bfloat16_rn(__bfloat162float(xe[q]) > 0.0f ? acc[q] : 0.0f);
+        *reinterpret_cast<uint4*>(g + (size_t)pix * Cin + c0) = *reinterpret_cast<uint4*>(o);
+    }
+}
+
+// out[r] = [ a[r][0 .. wa) | b[r][0 .. wb) ]  (bf16 rows side by side).
+__global__ void k_sg_hcat(const __nv_bfloat16* __restrict__ a, int wa, const __nv_bfloat16* __restrict__ b, int wb,
+                          int rows, __nv_bfloat16* __restrict__ out)
+{
+    const int w = wa + wb;
+    const long long n = (long long)rows * w;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long r = t / w;
+        const int c = (int)(t % w);
+        out[t] = c < wa ? a[r * wa + c] : b[r * wb + c - wa];
+    }
+}
+
+// out[r][c] = bf16(dY[r][c] * (H[r][c] > 0)) for c < cols, with row strides
+// (ReLU backward through the leading columns of a wider gradient).
+__global__ void k_sg_relu_grad_cols(const float* __restrict__ dY, int ldy, const __nv_bfloat16* __restrict__ H,
+                                    int ldh, int rows, int cols, __nv_bfloat16* __restrict__ out)
+{
+    const long long n = (long long)rows * cols;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long r = t / cols;
+        const int c = (int)(t % cols);
+        out[t] = __float2bfloat16_rn(__bfloat162float(H[r * ldh + c]) > 0.0f ? dY[r * ldy + c] : 0.0f);
+    }
+}
+
+// out[c][r] = in[r][c] (f32, 32 x 32 tiles through shared memory).
+__global__ void k_sg_transpose_f32(const float* __restrict__ in, int R, int C, float* __restrict__ out)
+{
+    __shared__ float t[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;   // row tiles on x (up to 2^31 - 1)
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r < R && c < C) t[k][threadIdx.x] = in[(size_t)r * C + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < R && c < C) out[(size_t)c * R + r] = t[threadIdx.x][k];
     }
 }
 
@@ -408,17 +586,22 @@ cudaError_t launch_gemm_tiles(const void* A, const void* B, float* C, void* Cb, 
 }  // namespace
 
 // Tile width: 256 columns when N allows it and the grid still covers the
-// SMs (148 on B200) at least once, else 128.
+// SMs (148 on B200) at least once, 64 when N is not a multiple of 128,
+// else 128.  SGB_GEMM_BN (64, 128, 256) forces a width that divides N.
 cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, const float* bias, int M, int N,
                              int K, int relu, int* err, cudaStream_t st)
 {
-    if (M <= 0 || N <= 0 || K <= 0 || M % kTm || N % 128 || K % kTk) return cudaErrorInvalidValue;
-    const char* force = getenv("SGB_GEMM_BN");
-    int bn = (N % 256 == 0 && (long long)(M / kTm) * (N / 256) >= 148) ? 256 : 128;
-    if (force && atoi(force) == 128) bn = 128;
-    if (force && atoi(force) == 256 && N % 256 == 0) bn = 256;
-    return bn == 256 ? launch_gemm_tiles<256>(A, B, C, Cb, bias, M, N, K, relu, err, st)
-                     : launch_gemm_tiles<128>(A, B, C, Cb, bias, M, N, K, relu, err, st);
+    if (M <= 0 || N <= 0 || K <= 0 || M % kTm || N % 64 || K % kTk) return cudaErrorInvalidValue;
+    int bn = N % 128 ? 64 : (N % 256 == 0 && (long long)(M / kTm) * (N / 256) >= 148) ? 256 : 128;
+    if (const char* force = getenv("SGB_GEMM_BN")) {
+        const int f = atoi(force);
+        if ((f == 64 || f == 128 || f == 256) && N % f == 0) bn = f;
+    }
+    switch (bn) {
+    case 256: return launch_gemm_tiles<256>(A, B, C, Cb, bias, M, N, K, relu, err, st);
+    case 128: return launch_gemm_tiles<128>(A, B, C, Cb, bias, M, N, K, relu, err, st);
+    default: return launch_gemm_tiles<64>(A, B, C, Cb, bias, M, N, K, relu, err, st);
+    }
 }
 
 }  // namespace sgb
@@ -479,7 +662,8 @@ int solar_gpu_sg_relu_grad(const float* dY, const void* H_bf16, long long n, voi
 int solar_gpu_sg_transpose(const void* in_bf16, int R, int C, void* out_bf16, void* stream)
 {
     if (R <= 0 || C <= 0) return 0;
-    sgb::k_sg_transpose<<<dim3((C + 31) / 32, (R + 31) / 32), dim3(32, 8), 0, (cudaStream_t)stream>>>(
+    if ((C + 31) / 32 > 65535) { sgb::set_last_error("transpose: C < 2^21"); return -1; }
+    sgb::k_sg_transpose<<<dim3((R + 31) / 32, (C + 31) / 32), dim3(32, 8), 0, (cudaStream_t)stream>>>(
         (const __nv_bfloat16*)in_bf16, R, C, (__nv_bfloat16*)out_bf16);
     return sg_status(cudaSuccess);
 }
@@ -487,7 +671,11 @@ int solar_gpu_sg_transpose(const void* in_bf16, int R, int C, void* out_bf16, vo
 int solar_gpu_sg_colsum(const void* in_bf16, int R, int C, float* out, void* stream)
 {
     if (R <= 0 || C <= 0) return 0;
-    sgb::k_sg_colsum<<<(C + 127) / 128, 128, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in_bf16, R, C, out);
+    const int rpb = std::max(64, (R + 1023) / 1024);
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * (size_t)C, (cudaStream_t)stream);
+    if (e != cudaSuccess) return sg_status(e);
+    sgb::k_sg_colsum<<<dim3((C + 127) / 128, (R + rpb - 1) / rpb), 128, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)in_bf16, R, C, rpb, out);
     return sg_status(cudaSuccess);
 }
 
@@ -498,6 +686,84 @@ int solar_gpu_sg_adam(float* p, const float* g, float* m, float* v, long long n,
     const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
     sgb::k_sg_adam<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2,
                                                                   (__nv_bfloat16*)p_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_coarse(const float* grid, int W, int H, float* out, void* stream)
+{
+    if (W <= 0 || H <= 0) return 0;
+    const int Wc = (W + sgb::kCoarse - 1) / sgb::kCoarse, Hc = (H + sgb::kCoarse - 1) / sgb::kCoarse;
+    sgb::k_sg_coarse<<<(Wc * Hc + 255) / 256, 256, 0, (cudaStream_t)stream>>>(grid, W, H, Wc, Hc, out);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_image(const float* grid, const float* coarse, int W, int H, int T, const int* pixel_parent,
+                       const float* wall_z, const float* slopes, const float* aspects, const int* voxels, int M,
+                       void* img_bf16, void* nrm_bf16, void* stream)
+{
+    if (M <= 0) return 0;
+    if (M > 65535) { sgb::set_last_error("image: M <= 65535"); return -1; }
+    sgb::k_sg_image<<<dim3(4, M), 256, 0, (cudaStream_t)stream>>>(grid, coarse, W, H, T, pixel_parent, wall_z, slopes,
+                                                                  aspects, voxels, M, (__nv_bfloat162*)img_bf16,
+                                                                  (__nv_bfloat16*)nrm_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_im2col(const void* X_bf16, int B, int Hi, int Wi, int Cin, int Kp, void* cols_bf16, void* stream)
+{
+    if (B <= 0) return 0;
+    if (Hi % 2 || Wi % 2 || Cin <= 0 || Kp % 64 || Kp < 16 * Cin || (Cin % 8 && Cin > 4)) {
+        sgb::set_last_error("im2col: even sides, Kp % 64 == 0, Kp >= 16 Cin, Cin % 8 == 0 or Cin <= 4");
+        return -1;
+    }
+    const long long n = (long long)B * (Hi / 2) * (Wi / 2) * (Kp / 8);
+    sgb::k_sg_im2col<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)X_bf16, B, Hi, Wi, Cin, Kp,
+                                                                     (__nv_bfloat16*)cols_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_col2im_relu(const float* dcols, const void* X_bf16, int B, int Hi, int Wi, int Cin, int Kp,
+                             void* g_bf16, void* stream)
+{
+    if (B <= 0) return 0;
+    if (Hi % 2 || Wi % 2 || Cin % 8 || Kp % 64 || Kp < 16 * Cin) {
+        sgb::set_last_error("col2im: even sides, Cin % 8 == 0, Kp % 64 == 0, Kp >= 16 Cin");
+        return -1;
+    }
+    const long long n = (long long)B * Hi * Wi * (Cin / 8);
+    sgb::k_sg_col2im_relu<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>(dcols, (const __nv_bfloat16*)X_bf16, B, Hi,
+                                                                          Wi, Cin, Kp, (__nv_bfloat16*)g_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_hcat(const void* a_bf16, int wa, const void* b_bf16, int wb, int rows, void* out_bf16, void* stream)
+{
+    const long long n = (long long)rows * (wa + wb);
+    if (n <= 0) return 0;
+    sgb::k_sg_hcat<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)a_bf16, wa,
+                                                                   (const __nv_bfloat16*)b_bf16, wb, rows,
+                                                                   (__nv_bfloat16*)out_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_relu_grad_cols(const float* dY, int ldy, const void* H_bf16, int ldh, int rows, int cols,
+                                void* out_bf16, void* stream)
+{
+    const long long n = (long long)rows * cols;
+    if (n <= 0) return 0;
+    if (cols > ldy || cols > ldh) { sgb::set_last_error("relu_grad_cols: cols > stride"); return -1; }
+    sgb::k_sg_relu_grad_cols<<<sg_blocks(n), 256, 0, (cudaStream_t)stream>>>(dY, ldy, (const __nv_bfloat16*)H_bf16,
+                                                                             ldh, rows, cols,
+                                                                             (__nv_bfloat16*)out_bf16);
+    return sg_status(cudaSuccess);
+}
+
+int solar_gpu_sg_transpose_f32(const float* in, int R, int C, float* out, void* stream)
+{
+    if (R <= 0 || C <= 0) return 0;
+    if ((C + 31) / 32 > 65535) { sgb::set_last_error("transpose: C < 2^21"); return -1; }
+    sgb::k_sg_transpose_f32<<<dim3((R + 31) / 32, (C + 31) / 32), dim3(32, 8), 0, (cudaStream_t)stream>>>(in, R, C,
+                                                                                                        out);
     return sg_status(cudaSuccess);
 }
 

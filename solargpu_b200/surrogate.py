@@ -1,18 +1,25 @@
-"""Sky-bin visibility surrogate: a BF16 MLP on the tcgen05 GEMM.
+"""Sky-bin visibility surrogate: a BF16 conv net on the tcgen05 GEMM.
 
 For a voxel, the model predicts its 265 sun-bin shadow bits (the DDA's
-shadow words: 1 = a ray toward that bin hits terrain) from the 64 x 64
-heights around its pixel (relative to the voxel's base height, / 50 m) and
-its normal:
+shadow words: 1 = a ray toward that bin hits terrain).  Two inputs:
 
-    features (4099, zero-padded to 4224) -> 512 -> 512 -> 512 -> 384 logits
-    (the first `active` columns are the sun bins), ReLU between layers.
+* conv model (the default): a 64 x 64 x 2 image around the voxel, channel 0
+  the 1 m cell heights, channel 1 the maxima of 8 x 8-cell context cells
+  (a 512 m window, so that long low-sun shadows are in view), both relative
+  to the voxel's base height / 50 m; and its normal.  Four 4 x 4, stride-2
+  convolutions (64, 64, 128, 128 channels, ReLU; 64 -> 32 -> 16 -> 8 -> 4
+  pixels), the 4 x 4 x 128 map and the normal (2048 + 64 columns) into
+  512 -> 512 -> 512 -> 384 logits;
+* MLP model (`conv=None`): the 64 x 64 heights and the normal, zero-padded
+  to 4224 columns, into the same MLP.
 
-Every matrix product, forward and backward, runs on the tensor cores through
-`solar_gpu_gemm_bf16` (bf16 operands, f32 accumulation in TMEM); features,
-labels, the loss, ReLU backward, transposes, bias sums and Adam are small
-CUDA kernels of the library.  Master weights and Adam moments are FP32,
-the GEMMs read bf16 copies.
+The first `active` logits are the sun bins; ReLU between layers.  Every
+product, forward and backward, runs on the tensor cores through
+`solar_gpu_gemm_bf16` (bf16 operands, f32 accumulation in TMEM); a
+convolution is im2col + GEMM, its input gradient GEMM + col2im (fused with
+the ReLU mask below it).  Images, labels, the loss, transposes, bias sums
+and Adam are small CUDA kernels of the library.  Master weights and Adam
+moments are FP32, the GEMMs read bf16 copies.
 
 `predict_with_fallback` is the guarded use: bits for every voxel from the
 model, then per 256 x 256-cell tile a random sample of voxels traced exactly
@@ -31,8 +38,11 @@ import numpy as np
 
 from . import api
 
-FEAT = 4224      # 64 * 64 + 3, padded to a multiple of 128
+FEAT = 4224      # 64 * 64 + 3, padded to a multiple of 128 (MLP model)
 OUTW = 384       # >= 265 active sun bins, a multiple of 128
+CONV = (64, 64, 128, 128)   # channels of the four stride-2 convolutions
+IMG = 64         # image side (pixels); 2 channels
+NRM = 64         # normal columns (3 used)
 
 
 def _lib():
@@ -46,6 +56,13 @@ def _lib():
         L.solar_gpu_sg_transpose.argtypes = [vp, i, i, vp, vp]
         L.solar_gpu_sg_colsum.argtypes = [vp, i, i, vp, vp]
         L.solar_gpu_sg_adam.argtypes = [vp, vp, vp, vp, ll, f, f, f, f, i, vp, vp]
+        L.solar_gpu_sg_coarse.argtypes = [vp, i, i, vp, vp]
+        L.solar_gpu_sg_image.argtypes = [vp, vp, i, i, i, vp, vp, vp, vp, vp, i, vp, vp, vp]
+        L.solar_gpu_sg_im2col.argtypes = [vp, i, i, i, i, i, vp, vp]
+        L.solar_gpu_sg_col2im_relu.argtypes = [vp, vp, i, i, i, i, i, vp, vp]
+        L.solar_gpu_sg_hcat.argtypes = [vp, i, vp, i, i, vp, vp]
+        L.solar_gpu_sg_relu_grad_cols.argtypes = [vp, i, vp, i, i, i, vp, vp]
+        L.solar_gpu_sg_transpose_f32.argtypes = [vp, i, i, vp, vp]
         L.solar_gpu_trace_shadow_subset.argtypes = [vp, C.POINTER(api.SceneDesc), vp, i, vp, C.POINTER(i), vp]
         L._sg_bound = True
     return L
@@ -63,16 +80,49 @@ def _t(torch, x):
     return out
 
 
+def _t32(torch, x):
+    """Transpose of a 2-D f32 CUDA tensor through the library kernel."""
+    R, Cc = x.shape
+    out = torch.empty(Cc, R, dtype=torch.float32, device=x.device)
+    api._check(_lib().solar_gpu_sg_transpose_f32(_p(x), R, Cc, _p(out), None))
+    return out
+
+
+def _round_up(x: int, m: int) -> int:
+    return (x + m - 1) // m * m
+
+
 class Surrogate:
+    """conv: channels of the stride-2 convolutions (None: MLP on `feat`
+    flat features).  Parameters W[l] / b[l] run over the convolutions
+    (W [Cout][Kp], Kp = 16 Cin rounded up to 128) then the MLP layers."""
+
     def __init__(self, active: int, hidden: int = 512, layers: int = 3, feat: int = FEAT, outw: int = OUTW,
-                 seed: int = 0, device: int = 0):
+                 seed: int = 0, device: int = 0, conv: tuple | None = CONV):
         import torch
         self.torch = torch
         self.dev = torch.device("cuda", device)
-        self.active, self.feat, self.outw = active, feat, outw
-        self.dims = [feat] + [hidden] * layers + [outw]
+        self.active, self.outw = active, outw
+        self.conv = tuple(conv) if conv else ()
         g = torch.Generator(device="cpu").manual_seed(seed)
         self.W, self.b = [], []
+        self.kp, self.sides, self.cins = [], [], []
+        side, cin = IMG, 2
+        for cout in self.conv:
+            if side % 2 or cout % 64:
+                raise ValueError("conv: even image sides and channels multiple of 64")
+            kp = _round_up(16 * cin, 128)
+            w = torch.zeros(cout, kp)
+            w[:, :16 * cin] = torch.randn(cout, 16 * cin, generator=g) * math.sqrt(2.0 / (16 * cin))
+            self.W.append(w.to(self.dev))
+            self.b.append(torch.zeros(cout, device=self.dev))
+            self.kp.append(kp)
+            self.sides.append(side)
+            self.cins.append(cin)
+            side, cin = side // 2, cout
+        self.feat = side * side * cin + NRM if self.conv else feat
+        self.flat = side * side * cin
+        self.dims = [self.feat] + [hidden] * layers + [outw]
         for a, o in zip(self.dims[:-1], self.dims[1:]):
             self.W.append((torch.randn(o, a, generator=g) * math.sqrt(2.0 / a)).to(self.dev))
             self.b.append(torch.zeros(o, device=self.dev))
@@ -85,14 +135,32 @@ class Surrogate:
 
     # -- data -----------------------------------------------------------------
 
-    def features(self, scene, dev: dict, voxels):
+    def inputs(self, scene, dev: dict, voxels) -> tuple:
+        """Model inputs of the listed voxels (device int32 ids): (image,
+        normal) for the conv model, (features,) for the MLP model."""
         torch = self.torch
         M = voxels.numel()
-        out = torch.empty(M, self.feat, dtype=torch.bfloat16, device=self.dev)
-        api._check(_lib().solar_gpu_sg_features(_p(dev["grid"]), scene.width, scene.height, scene.num_top,
-                                                _p(dev["pixel_parent"]), _p(dev["wall_z"]), _p(dev["slopes"]),
-                                                _p(dev["aspects"]), _p(voxels), M, self.feat, _p(out), None))
-        return out
+        if not self.conv:
+            out = torch.empty(M, self.feat, dtype=torch.bfloat16, device=self.dev)
+            api._check(_lib().solar_gpu_sg_features(_p(dev["grid"]), scene.width, scene.height, scene.num_top,
+                                                    _p(dev["pixel_parent"]), _p(dev["wall_z"]), _p(dev["slopes"]),
+                                                    _p(dev["aspects"]), _p(voxels), M, self.feat, _p(out), None))
+            return (out,)
+        if "coarse" not in dev:
+            wc, hc = (scene.width + 7) // 8, (scene.height + 7) // 8
+            dev["coarse"] = torch.empty(hc * wc, dtype=torch.float32, device=self.dev)
+            api._check(_lib().solar_gpu_sg_coarse(_p(dev["grid"]), scene.width, scene.height, _p(dev["coarse"]), None))
+        img = torch.empty(M, IMG, IMG, 2, dtype=torch.bfloat16, device=self.dev)
+        nrm = torch.empty(M, NRM, dtype=torch.bfloat16, device=self.dev)
+        api._check(_lib().solar_gpu_sg_image(_p(dev["grid"]), _p(dev["coarse"]), scene.width, scene.height,
+                                             scene.num_top, _p(dev["pixel_parent"]), _p(dev["wall_z"]),
+                                             _p(dev["slopes"]), _p(dev["aspects"]), _p(voxels), M, _p(img), _p(nrm),
+                                             None))
+        return img, nrm
+
+    def features(self, scene, dev: dict, voxels):
+        """Flat features of the MLP model."""
+        return self.inputs(scene, dev, voxels)[0]
 
     def labels(self, shadow_dev, words32: int, voxels):
         torch = self.torch
@@ -104,39 +172,77 @@ class Surrogate:
 
     # -- model ----------------------------------------------------------------
 
-    def forward(self, X):
-        """Activations (bf16, ReLU applied) of every hidden layer and the f32 logits."""
+    def forward(self, X, nrm=None):
+        """GEMM inputs of every layer (im2col columns for the convolutions,
+        activations for the MLP), the bf16 post-ReLU outputs of every hidden
+        layer, and the f32 logits."""
         torch = self.torch
-        acts = [X]
+        L = _lib()
+        ins, outs = [], []
         h = X
-        for l in range(len(self.Wb) - 1):
-            hn = torch.empty(h.shape[0], self.dims[l + 1], dtype=torch.bfloat16, device=self.dev)
+        B = X.shape[0]
+        for l, cout in enumerate(self.conv):
+            side, cin, kp = self.sides[l], self.cins[l], self.kp[l]
+            rows = B * (side // 2) ** 2
+            cols = torch.empty(rows, kp, dtype=torch.bfloat16, device=self.dev)
+            api._check(L.solar_gpu_sg_im2col(_p(h), B, side, side, cin, kp, _p(cols), None))
+            y = torch.empty(rows, cout, dtype=torch.bfloat16, device=self.dev)
+            api.gemm_bf16(cols, self.Wb[l], out_bf16=y, bias=self.b[l], relu=True)
+            ins.append(cols)
+            outs.append(y)
+            h = y
+        if self.conv:
+            flat = torch.empty(B, self.feat, dtype=torch.bfloat16, device=self.dev)
+            api._check(L.solar_gpu_sg_hcat(_p(h), self.flat, _p(nrm), NRM, B, _p(flat), None))
+            h = flat
+        nc = len(self.conv)
+        for l in range(nc, len(self.Wb) - 1):
+            hn = torch.empty(B, self.dims[l - nc + 1], dtype=torch.bfloat16, device=self.dev)
             api.gemm_bf16(h, self.Wb[l], out_bf16=hn, bias=self.b[l], relu=True)
-            acts.append(hn)
+            ins.append(h)
+            outs.append(hn)
             h = hn
+        ins.append(h)
         Z = api.gemm_bf16(h, self.Wb[-1], bias=self.b[-1])
-        return acts, Z
+        return ins, outs, Z
 
-    def gradients(self, X, Y):
+    def gradients(self, X, Y, nrm=None):
         """Loss and the gradients of every weight and bias (f32)."""
         torch = self.torch
-        M = X.shape[0]
-        acts, Z = self.forward(X)
+        L = _lib()
+        B = X.shape[0]
+        ins, outs, Z = self.forward(X, nrm)
         loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
-        g = torch.empty(M, self.outw, dtype=torch.bfloat16, device=self.dev)
-        api._check(_lib().solar_gpu_sg_bce(_p(Z), _p(Y), M, self.outw, self.active, _p(g), _p(loss), None))
+        g = torch.empty(B, self.outw, dtype=torch.bfloat16, device=self.dev)
+        api._check(L.solar_gpu_sg_bce(_p(Z), _p(Y), B, self.outw, self.active, _p(g), _p(loss), None))
+        nc = len(self.conv)
         dW = [None] * len(self.W)
         db = [None] * len(self.W)
         for l in range(len(self.W) - 1, -1, -1):
-            a = acts[l]
-            dW[l] = api.gemm_bf16(_t(torch, g), _t(torch, a))                 # [out, in] = g^T a
-            db[l] = torch.empty(self.dims[l + 1], dtype=torch.float32, device=self.dev)
-            api._check(_lib().solar_gpu_sg_colsum(_p(g), M, self.dims[l + 1], _p(db[l]), None))
-            if l > 0:
-                dA = api.gemm_bf16(g, _t(torch, self.Wb[l]))                  # [M, in] = g W
-                gn = torch.empty(M, self.dims[l], dtype=torch.bfloat16, device=self.dev)
-                api._check(_lib().solar_gpu_sg_relu_grad(_p(dA), _p(a), dA.numel(), _p(gn), None))
-                g = gn
+            a = ins[l]
+            rows, n_out = g.shape
+            if l < nc:
+                dW[l] = _t32(torch, api.gemm_bf16(_t(torch, a), _t(torch, g)))   # ([K, rows] [rows, N])^T
+            else:
+                dW[l] = api.gemm_bf16(_t(torch, g), _t(torch, a))                # [N, K] = g^T a
+            db[l] = torch.empty(n_out, dtype=torch.float32, device=self.dev)
+            api._check(L.solar_gpu_sg_colsum(_p(g), rows, n_out, _p(db[l]), None))
+            if l == 0:
+                break
+            dA = api.gemm_bf16(g, _t(torch, self.Wb[l]))                         # [rows, K] = g W
+            below = outs[l - 1]
+            if l > nc:                  # MLP layer over an MLP layer
+                gn = torch.empty(rows, dA.shape[1], dtype=torch.bfloat16, device=self.dev)
+                api._check(L.solar_gpu_sg_relu_grad(_p(dA), _p(below), dA.numel(), _p(gn), None))
+            elif l == nc:               # first MLP layer over the last convolution
+                gn = torch.empty_like(below)    # [B * 16][128] = [B][flat]
+                api._check(L.solar_gpu_sg_relu_grad_cols(_p(dA), self.feat, _p(below), self.flat, B, self.flat,
+                                                         _p(gn), None))
+            else:                       # convolution over a convolution
+                side, cin, kp = self.sides[l], self.cins[l], self.kp[l]
+                gn = torch.empty(B * side * side, cin, dtype=torch.bfloat16, device=self.dev)
+                api._check(L.solar_gpu_sg_col2im_relu(_p(dA), _p(below), B, side, side, cin, kp, _p(gn), None))
+            g = gn
         return float(loss.item()), dW, db
 
     def apply(self, dW, db, lr: float = 1e-3, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
@@ -151,25 +257,27 @@ class Surrogate:
 
     def train(self, data: list, steps: int, batch: int = 1024, lr: float = 1e-3, seed: int = 0, log_every: int = 0):
         """data: (scene, dev arrays, shadow words on the device, words32) per
-        training scene; batches of `batch` voxels drawn uniformly."""
+        training scene; batches of `batch` voxels (a multiple of 128) drawn
+        uniformly."""
         torch = self.torch
         rng = np.random.default_rng(seed)
         losses = []
         for it in range(steps):
             scene, dev, shadow, words32 = data[it % len(data)]
             vox = torch.from_numpy(rng.integers(0, scene.num_total, batch, dtype=np.int32)).to(self.dev)
-            X = self.features(scene, dev, vox)
             Y = self.labels(shadow, words32, vox)
-            loss, dW, db = self.gradients(X, Y)
+            inp = self.inputs(scene, dev, vox)
+            loss, dW, db = self.gradients(inp[0], Y, *inp[1:])
             self.apply(dW, db, lr)
             losses.append(loss)
             if log_every and (it + 1) % log_every == 0:
                 print(f"step {it + 1}: loss {np.mean(losses[-log_every:]):.4f}", flush=True)
         return losses
 
-    def predict_bits(self, scene, dev: dict, voxels, batch: int = 16384):
+    def predict_bits(self, scene, dev: dict, voxels, batch: int | None = None):
         """Predicted shadow words [n][ceil(active/32)] (uint32, on the device)."""
         torch = self.torch
+        batch = batch or (4096 if self.conv else 16384)
         n = voxels.numel()
         words = (self.active + 31) // 32
         out = torch.zeros(n, words, dtype=torch.int64, device=self.dev)
@@ -180,7 +288,7 @@ class Surrogate:
             pad = (-m) % 128
             if pad:
                 v = torch.cat([v, v[:1].expand(pad)])
-            _, Z = self.forward(self.features(scene, dev, v))
+            _, _, Z = self.forward(*self.inputs(scene, dev, v))
             bits = (Z[:m, :self.active] > 0).to(torch.int64)
             bits = torch.nn.functional.pad(bits, (0, 32 * words - self.active))
             out[i0:i0 + m] = (bits.view(m, words, 32) << shifts).sum(-1)
@@ -244,19 +352,22 @@ def main(argv=None) -> int:
     """Train on some synthetic cities, then the guarded prediction on another
     against the exact tracer (the ablation):
 
-        python -m solargpu_b200.surrogate [--train dsm256,dsm512] [--test dsm1024] [--steps 3000]
+        python -m solargpu_b200.surrogate [--model conv|mlp] [--train dsm256,dsm512] [--test dsm1024]
+                                          [--steps 3000]
     """
     import argparse
     import json
     import torch
     from . import inputs
     ap = argparse.ArgumentParser(description="sky-bin visibility surrogate: train and ablation")
+    ap.add_argument("--model", choices=("conv", "mlp"), default="conv")
     ap.add_argument("--train", default="dsm256,dsm512")
     ap.add_argument("--test", default="dsm1024")
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--max-err", type=float, default=0.02)
+    ap.add_argument("--log-every", type=int, default=0)
     ap.add_argument("--gemm-only", type=int, default=0, metavar="SIZE",
                     help="only time the tensor-core GEMM on SIZE x SIZE x SIZE (profiling)")
     a = ap.parse_args(argv)
@@ -278,11 +389,12 @@ def main(argv=None) -> int:
             r = ctx.trace(s, d, neighbor_format=0)
             data.append((s, d, torch.from_numpy(r["shadow"].view(np.int32)).cuda(), r["shadow_words"]))
             active = r["active_bins"]
-        model = Surrogate(active=active, seed=0)
+        model = Surrogate(active=active, seed=0, conv=CONV if a.model == "conv" else None)
         t0 = time.perf_counter()
-        losses = model.train(data, a.steps, a.batch, a.lr)
+        losses = model.train(data, a.steps, a.batch, a.lr, log_every=a.log_every)
         torch.cuda.synchronize()
-        res["train"] = {"scenes": a.train, "steps": a.steps, "batch": a.batch, "s": round(time.perf_counter() - t0, 2),
+        res["train"] = {"model": a.model, "parameters": int(sum(w.numel() + b.numel() for w, b in zip(model.W, model.b))),
+                        "scenes": a.train, "steps": a.steps, "batch": a.batch, "s": round(time.perf_counter() - t0, 2),
                         "loss_first100": float(np.mean(losses[:100])), "loss_last100": float(np.mean(losses[-100:]))}
         s, d = staged(a.test)
         allv = torch.arange(s.num_total, dtype=torch.int32, device="cuda")
