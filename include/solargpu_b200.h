@@ -107,6 +107,14 @@ void solar_gpu_destroy(solar_gpu_context* ctx);
    are no longer available afterwards. */
 int solar_gpu_release(solar_gpu_context* ctx);
 
+/* No counterpart in the reference.  Caps the device bytes the context's
+   buffers may hold (0: no cap; the default), e.g. for several contexts
+   sharing one GPU.  A call that would pass the cap returns SOLAR_GPU_ERR_OOM
+   before allocating, and the context stays usable; the tracer's automatic
+   chunk is sized within the cap.  memory_held: bytes held now. */
+int solar_gpu_set_memory_limit(solar_gpu_context* ctx, long long bytes);
+long long solar_gpu_memory_held(solar_gpu_context* ctx);
+
 /* Scene description.  For solar_gpu_run_host the array pointers are host
    pointers; for solar_gpu_run_device and solar_gpu_trace the per-cell and
    per-voxel arrays (grid, pixel_parent, wall_z, slopes, aspects) are device
@@ -238,6 +246,14 @@ int solar_gpu_trace_shadow_subset(solar_gpu_context* ctx, const solar_gpu_scene*
    K of 64.  Synchronous on `stream`. */
 int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N,
                         int K, int relu, void* stream);
+
+/* No counterpart in the reference.  Self-test of the device-side bounded
+   waits: one GEMM tile whose operand loads are withheld, so that its MMA
+   thread's wait for them runs out (about 1 s); the kernel records the error
+   and exits normally.  Returns what any expired wait returns,
+   SOLAR_GPU_ERR_DEVICE_CHECK with "a bounded wait expired" as the last
+   error; the device stays usable. */
+int solar_gpu_selftest_bounded_wait(void* stream);
 
 /* Surrogate training/inference kernels (device pointers, bf16 = 2-byte
    bfloat16, row-major).  features: per voxel the 64 x 64 heights around its

@@ -85,6 +85,9 @@ def lib() -> C.CDLL:
         L.solar_gpu_destroy.argtypes = [vp]
         L.solar_gpu_destroy.restype = None
         L.solar_gpu_release.argtypes = [vp]
+        L.solar_gpu_set_memory_limit.argtypes = [vp, C.c_longlong]
+        L.solar_gpu_memory_held.argtypes = [vp]
+        L.solar_gpu_memory_held.restype = C.c_longlong
         L.solar_gpu_default_options.argtypes = [C.POINTER(Options)]
         L.solar_gpu_default_options.restype = None
         L.solar_gpu_run_host.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), vp]
@@ -229,6 +232,14 @@ class Context:
     def release(self):
         """Frees the device buffers kept between calls (solar_gpu_release)."""
         _check(lib().solar_gpu_release(self.h))
+
+    def set_memory_limit(self, nbytes: int):
+        """Caps the device bytes this context's buffers may hold (0: no cap);
+        a call that would pass it raises SolarGPUError (SOLAR_GPU_ERR_OOM)."""
+        _check(lib().solar_gpu_set_memory_limit(self.h, int(nbytes)))
+
+    def memory_held(self) -> int:
+        return int(lib().solar_gpu_memory_held(self.h))
 
     def __enter__(self):
         return self

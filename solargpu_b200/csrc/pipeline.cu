@@ -92,6 +92,7 @@ struct solar_gpu_context {
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
+    long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
     long long csr_total = 0, barle_total = 0;
@@ -110,27 +111,57 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
+static constexpr int kNumBufs = 65;
+extern "C" {
+static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
+}
+
 namespace {
 
-int ensure(DevBuf& b, size_t bytes)
+// Device bytes held by the context's buffers.
+size_t held_bytes(solar_gpu_context* c)
+{
+    DevBuf* bufs[kNumBufs];
+    all_bufs(c, bufs);
+    size_t h = 0;
+    for (DevBuf* b : bufs) h += b->cap;
+    return h;
+}
+
+// Refuses (SOLAR_GPU_ERR_OOM, nothing allocated) when holding `extra` more
+// bytes would pass the context's memory limit.
+int check_limit(solar_gpu_context* c, size_t extra)
+{
+    if (c->mem_limit <= 0) return SOLAR_GPU_OK;
+    const size_t held = held_bytes(c);
+    if (held + extra > (size_t)c->mem_limit)
+        return fail(SOLAR_GPU_ERR_OOM, "device memory limit of %lld bytes: %zu held, %zu more needed", c->mem_limit,
+                    held, extra);
+    return SOLAR_GPU_OK;
+}
+
+int ensure(solar_gpu_context* c, DevBuf& b, size_t bytes)
 {
     if (bytes == 0) bytes = 16;
     if (b.cap >= bytes) return SOLAR_GPU_OK;
+    const size_t cap = (bytes + 255) & ~(size_t)255;
+    RK(check_limit(c, cap - b.cap));
     if (b.p) CK(cudaFree(b.p));
     b.p = nullptr;
     b.cap = 0;
-    const size_t cap = (bytes + 255) & ~(size_t)255;
     CK(cudaMalloc(&b.p, cap));
     b.cap = cap;
     return SOLAR_GPU_OK;
 }
 
-// Grows `b` to at least `bytes`, keeping the first `used` bytes.
-int ensure_keep(DevBuf& b, size_t bytes, size_t used, cudaStream_t st)
+// Grows `b` to at least `bytes`, keeping the first `used` bytes (old and new
+// buffers are both held during the copy).
+int ensure_keep(solar_gpu_context* c, DevBuf& b, size_t bytes, size_t used, cudaStream_t st)
 {
     if (b.cap >= bytes) return SOLAR_GPU_OK;
     void* np = nullptr;
     const size_t cap = ((bytes + bytes / 8) + 255) & ~(size_t)255;
+    RK(check_limit(c, cap));
     CK(cudaMalloc(&np, cap));
     if (used && b.p) CK(cudaMemcpyAsync(np, b.p, used, cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
@@ -241,14 +272,14 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
     const int D = (int)sky.dirs.size();
     const int Hd = (int)sky.hour_index.size();
     const int n_padded = ((Hd + 511) / 512) * 512 + 512;   // room for the widest hour block
-    RK(ensure(c->dirs, sizeof(DirEntry) * D));
-    RK(ensure(c->nudged, sizeof(float) * 2 * kHoursPerYear));
-    RK(ensure(c->dni, sizeof(float) * kHoursPerYear));
-    RK(ensure(c->dhi, sizeof(float) * kHoursPerYear));
-    RK(ensure(c->sun_dense, sizeof(int) * kHoursPerYear));
-    RK(ensure(c->hour_index, sizeof(int) * (Hd + 1)));
-    RK(ensure(c->table, sizeof(HourEntry) * n_padded));
-    RK(ensure(c->err, sizeof(int)));
+    RK(ensure(c, c->dirs, sizeof(DirEntry) * D));
+    RK(ensure(c, c->nudged, sizeof(float) * 2 * kHoursPerYear));
+    RK(ensure(c, c->dni, sizeof(float) * kHoursPerYear));
+    RK(ensure(c, c->dhi, sizeof(float) * kHoursPerYear));
+    RK(ensure(c, c->sun_dense, sizeof(int) * kHoursPerYear));
+    RK(ensure(c, c->hour_index, sizeof(int) * (Hd + 1)));
+    RK(ensure(c, c->table, sizeof(HourEntry) * n_padded));
+    RK(ensure(c, c->err, sizeof(int)));
     CK(cudaMemcpyAsync(c->dirs.p, sky.dirs.data(), sizeof(DirEntry) * D, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->nudged.p, sky.nudged.data(), sizeof(float) * 2 * kHoursPerYear, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->dni.p, s->direct_irradiance, sizeof(float) * kHoursPerYear, cudaMemcpyHostToDevice, st));
@@ -262,8 +293,8 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
                              as<int>(c->hour_index), Hd, n_padded, as<HourEntry>(c->table), st));
     }
     const int N = s->num_total_voxels;
-    RK(ensure(c->geo_n, sizeof(float4) * (size_t)N));
-    RK(ensure(c->geo_p, sizeof(float4) * (size_t)N));
+    RK(ensure(c, c->geo_n, sizeof(float4) * (size_t)N));
+    RK(ensure(c, c->geo_p, sizeof(float4) * (size_t)N));
     {
         KScope k(c, SOLAR_GPU_KT_SETUP);
         k_validate_parents<<<(N + 255) / 256, 256, 0, st>>>(s->pixel_parent, N, s->num_top_voxels, as<int>(c->err));
@@ -281,11 +312,11 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
     }
     {
         const long long npos = order_positions(s->grid_width, s->grid_height);
-        RK(ensure(c->order, sizeof(int) * (size_t)N));
-        RK(ensure(c->order_cnt, sizeof(int) * (size_t)npos));
-        RK(ensure(c->order_first, sizeof(int) * ((size_t)npos + 1)));
-        RK(ensure(c->order_cur, sizeof(long long) * ((size_t)npos + 1)));
-        RK(ensure(c->order_tmp, sizeof(long long) * scan_scratch_elems((int)npos)));
+        RK(ensure(c, c->order, sizeof(int) * (size_t)N));
+        RK(ensure(c, c->order_cnt, sizeof(int) * (size_t)npos));
+        RK(ensure(c, c->order_first, sizeof(int) * ((size_t)npos + 1)));
+        RK(ensure(c, c->order_cur, sizeof(long long) * ((size_t)npos + 1)));
+        RK(ensure(c, c->order_tmp, sizeof(long long) * scan_scratch_elems((int)npos)));
         KScope k(c, SOLAR_GPU_KT_SETUP);
         CK(launch_voxel_order(s->pixel_parent, N, s->num_top_voxels, s->grid_width, s->grid_height,
                               as<int>(c->order_cnt), as<int>(c->order_first), as<long long>(c->order_cur),
@@ -295,10 +326,16 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
     return SOLAR_GPU_OK;
 }
 
-long long auto_chunk(int N, int D)
+long long auto_chunk(solar_gpu_context* c, int N, int D)
 {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
+    if (c->mem_limit > 0) {
+        // under a memory limit: what the limit leaves, counting the raw buffer's current size as free
+        const size_t held = held_bytes(c) - c->raw.cap;
+        const size_t room = (size_t)c->mem_limit > held ? (size_t)c->mem_limit - held : 0;
+        if (room < free_b) free_b = room;
+    }
     // The raw hit rows (D ints per voxel) get at most 35 % of free memory.
     const double budget = 0.35 * (double)free_b;
     long long chunk = (long long)(budget / ((double)D * sizeof(int)));
@@ -312,7 +349,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
 {
     const int N = s->num_total_voxels;
     const int D = (int)sky.dirs.size();
-    const long long chunk = o->chunk_voxels > 0 ? (o->chunk_voxels < N ? o->chunk_voxels : N) : auto_chunk(N, D);
+    const long long chunk = o->chunk_voxels > 0 ? (o->chunk_voxels < N ? o->chunk_voxels : N) : auto_chunk(c, N, D);
     c->N = N;
     c->T = s->num_top_voxels;
     c->words32 = sky.words32 > 0 ? sky.words32 : 1;
@@ -320,19 +357,19 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     c->have_csr = want_csr;
     c->have_barle = want_barle;
     c->csr_total = c->barle_total = 0;
-    RK(ensure(c->shadow, sizeof(uint32_t) * (size_t)N * c->words32));
+    RK(ensure(c, c->shadow, sizeof(uint32_t) * (size_t)N * c->words32));
     CK(cudaMemsetAsync(c->shadow.p, 0, sizeof(uint32_t) * (size_t)N * c->words32, st));
-    RK(ensure(c->raw, sizeof(int) * (size_t)chunk * D));
-    RK(ensure(c->counts, sizeof(int) * (size_t)N));
-    RK(ensure(c->scan_tmp, sizeof(long long) * scan_scratch_elems((int)chunk)));
+    RK(ensure(c, c->raw, sizeof(int) * (size_t)chunk * D));
+    RK(ensure(c, c->counts, sizeof(int) * (size_t)N));
+    RK(ensure(c, c->scan_tmp, sizeof(long long) * scan_scratch_elems((int)chunk)));
     if (want_csr) {
-        RK(ensure(c->csr_off, sizeof(long long) * ((size_t)N + 1)));
-        RK(ensure(c->csr_ids, sizeof(int) * (size_t)N * 96));
+        RK(ensure(c, c->csr_off, sizeof(long long) * ((size_t)N + 1)));
+        RK(ensure(c, c->csr_ids, sizeof(int) * (size_t)N * 96));
     }
     if (want_barle) {
-        RK(ensure(c->barle_off, sizeof(long long) * ((size_t)N + 1)));
-        RK(ensure(c->barle_sizes, sizeof(int) * (size_t)N));
-        RK(ensure(c->barle_bytes, (size_t)N * 160));
+        RK(ensure(c, c->barle_off, sizeof(long long) * ((size_t)N + 1)));
+        RK(ensure(c, c->barle_sizes, sizeof(int) * (size_t)N));
+        RK(ensure(c, c->barle_bytes, (size_t)N * 160));
     }
     const DevScene ds = dev_scene(s);
     // Rows follow the visiting order (Morton-adjacent voxels share a warp, so
@@ -340,17 +377,17 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     // range of voxel indices) is traced in the visiting order of its voxels.
     const int* perm = nullptr;
     const int* inv = nullptr;
-    RK(ensure(c->order_inv, sizeof(int) * (size_t)N));
+    RK(ensure(c, c->order_inv, sizeof(int) * (size_t)N));
     if (chunk >= N) {
         CK(launch_invert(as<int>(c->order), N, as<int>(c->order_inv), st));
         perm = as<int>(c->order);
         inv = as<int>(c->order_inv);
         c->launches += 1;
     } else {
-        RK(ensure(c->chunk_perm, sizeof(int) * (size_t)chunk));
-        RK(ensure(c->chunk_flag, sizeof(int) * (size_t)N));
-        RK(ensure(c->chunk_pos, sizeof(long long) * ((size_t)N + 1)));
-        RK(ensure(c->chunk_tmp, sizeof(long long) * scan_scratch_elems(N)));
+        RK(ensure(c, c->chunk_perm, sizeof(int) * (size_t)chunk));
+        RK(ensure(c, c->chunk_flag, sizeof(int) * (size_t)N));
+        RK(ensure(c, c->chunk_pos, sizeof(long long) * ((size_t)N + 1)));
+        RK(ensure(c, c->chunk_tmp, sizeof(long long) * scan_scratch_elems(N)));
         perm = as<int>(c->chunk_perm);
         inv = as<int>(c->order_inv);
     }
@@ -385,7 +422,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
             long long total = 0;
             RK(read_ll(c, off + n, &total, st));
             const long long est = (long long)(total * frac_left * 1.05);
-            RK(ensure_keep(c->csr_ids, sizeof(int) * (size_t)(est > total ? est : total), sizeof(int) * (size_t)csr_total, st));
+            RK(ensure_keep(c, c->csr_ids, sizeof(int) * (size_t)(est > total ? est : total), sizeof(int) * (size_t)csr_total, st));
             {
                 KScope k(c, SOLAR_GPU_KT_CSR);
                 CK(launch_gather_csr(n, D, as<int>(c->raw), off, as<int>(c->csr_ids), inv, st));
@@ -404,7 +441,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
             long long total = 0;
             RK(read_ll(c, off + n, &total, st));
             const long long est = (long long)(total * frac_left * 1.05);
-            RK(ensure_keep(c->barle_bytes, (size_t)(est > total ? est : total), (size_t)barle_total, st));
+            RK(ensure_keep(c, c->barle_bytes, (size_t)(est > total ? est : total), (size_t)barle_total, st));
             {
                 KScope k(c, SOLAR_GPU_KT_BARLE);
                 CK(launch_barle_write(n, D, as<int>(c->raw), as<int>(c->counts) + v0, off,
@@ -451,8 +488,8 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
     const HourEntry* tab = as<HourEntry>(c->table);
     int* err = as<int>(c->err);
     if (o->reflection == SOLAR_GPU_REFL_ANNUAL) {
-        RK(ensure(c->sums, sizeof(double) * (size_t)N));
-        RK(ensure(c->out_f64, sizeof(double) * (size_t)N));
+        RK(ensure(c, c->sums, sizeof(double) * (size_t)N));
+        RK(ensure(c, c->out_f64, sizeof(double) * (size_t)N));
         {
             KScope k(c, SOLAR_GPU_KT_SOLAR);
             CK(launch_solar_sum(g, N, sh, c->words32, tab, Hd, as<double>(c->sums), st));
@@ -473,19 +510,19 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
     acc.f64 = nullptr;
     acc.f32 = acc.comp = nullptr;
     if (acc.mode == SOLAR_GPU_ACC_FP64) {
-        RK(ensure(c->acc_f64, sizeof(double) * (size_t)N));
+        RK(ensure(c, c->acc_f64, sizeof(double) * (size_t)N));
         acc.f64 = as<double>(c->acc_f64);
         CK(cudaMemsetAsync(acc.f64, 0, sizeof(double) * (size_t)N, st));
     } else {
-        RK(ensure(c->acc_f32, sizeof(float) * (size_t)N));
-        RK(ensure(c->acc_comp, sizeof(float) * (size_t)N));
+        RK(ensure(c, c->acc_f32, sizeof(float) * (size_t)N));
+        RK(ensure(c, c->acc_comp, sizeof(float) * (size_t)N));
         acc.f32 = as<float>(c->acc_f32);
         acc.comp = as<float>(c->acc_comp);
         CK(cudaMemsetAsync(acc.f32, 0, sizeof(float) * (size_t)N, st));
         CK(cudaMemsetAsync(acc.comp, 0, sizeof(float) * (size_t)N, st));
     }
     if (B == 1) {
-        RK(ensure(c->hourly, sizeof(float) * (size_t)N));
+        RK(ensure(c, c->hourly, sizeof(float) * (size_t)N));
         for (int j = 0; j < Hd; ++j) {
             {
                 KScope k(c, SOLAR_GPU_KT_SOLAR);
@@ -508,9 +545,9 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
             // Once per run: the nonzero weights of every list in visiting order,
             // then (V > 1) the merged union entries of each group of V voxels.
             const int V = o->group_size;
-            RK(ensure(c->w_cnt, sizeof(int) * (size_t)N));
-            RK(ensure(c->w_off, sizeof(long long) * ((size_t)N + 1)));
-            RK(ensure(c->w_tmp, sizeof(long long) * scan_scratch_elems(N)));
+            RK(ensure(c, c->w_cnt, sizeof(int) * (size_t)N));
+            RK(ensure(c, c->w_off, sizeof(long long) * ((size_t)N + 1)));
+            RK(ensure(c, c->w_tmp, sizeof(long long) * scan_scratch_elems(N)));
             {
                 KScope k(c, SOLAR_GPU_KT_GROUP);
                 CK(launch_weight_lists(0, g, N, T, nl, as<int>(c->order), as<int>(c->w_cnt), nullptr, nullptr,
@@ -521,8 +558,8 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
             long long Ew = 0;
             RK(read_ll(c, as<long long>(c->w_off) + N, &Ew, st));
             c->weighted_entries = Ew;
-            RK(ensure(c->w_cell, sizeof(int) * (size_t)(Ew + 1)));
-            RK(ensure(c->w_val, sizeof(float) * (size_t)(Ew + 1)));
+            RK(ensure(c, c->w_cell, sizeof(int) * (size_t)(Ew + 1)));
+            RK(ensure(c, c->w_val, sizeof(float) * (size_t)(Ew + 1)));
             {
                 KScope k(c, SOLAR_GPU_KT_GROUP);
                 CK(launch_weight_lists(1, g, N, T, nl, as<int>(c->order), nullptr, as<long long>(c->w_off),
@@ -539,10 +576,10 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 // each group are rewritten in place into union cells + slots,
                 // then the slot lists of each 4 consecutive voxels are merged
                 // and laid out chunk by chunk.
-                RK(ensure(c->tile_flag, sizeof(int) * (size_t)N));
-                RK(ensure(c->tile_pos, sizeof(long long) * ((size_t)N + 1)));
-                RK(ensure(c->tile_start, sizeof(int) * ((size_t)N + 1)));
-                RK(ensure(c->tile_slot, sizeof(unsigned short) * (size_t)(Ew + 1)));
+                RK(ensure(c, c->tile_flag, sizeof(int) * (size_t)N));
+                RK(ensure(c, c->tile_pos, sizeof(long long) * ((size_t)N + 1)));
+                RK(ensure(c, c->tile_start, sizeof(int) * ((size_t)N + 1)));
+                RK(ensure(c, c->tile_slot, sizeof(unsigned short) * (size_t)(Ew + 1)));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(launch_tile_groups(N, V, as<long long>(c->w_off), as<int>(c->tile_flag),
@@ -551,8 +588,8 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 }
                 long long NG = 0;
                 RK(read_ll(c, as<long long>(c->tile_pos) + N, &NG, st));
-                RK(ensure(c->tile_union, sizeof(int) * (size_t)(NG + 1)));
-                RK(ensure(c->tile_rows, sizeof(long long)));
+                RK(ensure(c, c->tile_union, sizeof(int) * (size_t)(NG + 1)));
+                RK(ensure(c, c->tile_rows, sizeof(long long)));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(launch_tile_build((int)NG, as<int>(c->tile_start), as<long long>(c->w_off),
@@ -561,10 +598,10 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 }
                 RK(read_ll(c, as<long long>(c->tile_rows), &c->staged_rows, st));
                 const int R = tile_rows_per_stage(B);
-                RK(ensure(c->tile_gcnt, sizeof(int) * (size_t)NG));
-                RK(ensure(c->tile_gnch, sizeof(int) * (size_t)NG));
-                RK(ensure(c->tile_gbase, sizeof(long long) * ((size_t)NG + 1)));
-                RK(ensure(c->tile_tbase, sizeof(long long) * ((size_t)NG + 1)));
+                RK(ensure(c, c->tile_gcnt, sizeof(int) * (size_t)NG));
+                RK(ensure(c, c->tile_gnch, sizeof(int) * (size_t)NG));
+                RK(ensure(c, c->tile_gbase, sizeof(long long) * ((size_t)NG + 1)));
+                RK(ensure(c, c->tile_tbase, sizeof(long long) * ((size_t)NG + 1)));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(launch_tile_layout(0, (int)NG, R, as<int>(c->tile_start), as<int>(c->tile_union),
@@ -579,9 +616,9 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 long long Em = 0, TC = 0;
                 RK(read_ll(c, as<long long>(c->tile_gbase) + NG, &Em, st));
                 RK(read_ll(c, as<long long>(c->tile_tbase) + NG, &TC, st));
-                RK(ensure(c->tile_erow, sizeof(unsigned short) * (size_t)(Em + 8)));
-                RK(ensure(c->tile_ew, sizeof(float4) * (size_t)(Em + 8)));
-                RK(ensure(c->tile_table, sizeof(int) * 20 * (size_t)(TC + 1)));
+                RK(ensure(c, c->tile_erow, sizeof(unsigned short) * (size_t)(Em + 8)));
+                RK(ensure(c, c->tile_ew, sizeof(float4) * (size_t)(Em + 8)));
+                RK(ensure(c, c->tile_table, sizeof(int) * 20 * (size_t)(TC + 1)));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(cudaMemsetAsync(c->tile_ew.p, 0, sizeof(float4) * (size_t)(Em + 8), st));
@@ -618,9 +655,9 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 tl.ew = as<float4>(c->tile_ew);
             } else {
                 const int G = group_count(N, V);
-                RK(ensure(c->grp_cnt, sizeof(int) * (size_t)G));
-                RK(ensure(c->grp_off, sizeof(long long) * ((size_t)G + 1)));
-                RK(ensure(c->grp_tmp, sizeof(long long) * scan_scratch_elems(G)));
+                RK(ensure(c, c->grp_cnt, sizeof(int) * (size_t)G));
+                RK(ensure(c, c->grp_off, sizeof(long long) * ((size_t)G + 1)));
+                RK(ensure(c, c->grp_tmp, sizeof(long long) * scan_scratch_elems(G)));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(launch_group_merge(0, V, N, as<long long>(c->w_off), as<int>(c->w_cell), as<float>(c->w_val),
@@ -630,8 +667,8 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 }
                 long long E = 0;
                 RK(read_ll(c, as<long long>(c->grp_off) + G, &E, st));
-                RK(ensure(c->grp_cell, sizeof(int) * (size_t)(E + 1)));
-                RK(ensure(c->grp_w, sizeof(float) * (size_t)(E + 1) * V));
+                RK(ensure(c, c->grp_cell, sizeof(int) * (size_t)(E + 1)));
+                RK(ensure(c, c->grp_w, sizeof(float) * (size_t)(E + 1) * V));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(launch_group_merge(1, V, N, as<long long>(c->w_off), as<int>(c->w_cell), as<float>(c->w_val),
@@ -647,7 +684,7 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         }
         // allocated after the once-per-run builds, whose intermediates may
         // have been released to make room (very large scenes)
-        RK(ensure(c->slab, sizeof(float) * (size_t)slab_rows * B));
+        RK(ensure(c, c->slab, sizeof(float) * (size_t)slab_rows * B));
         float* slab = as<float>(c->slab);
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
@@ -774,13 +811,13 @@ int run_lists_impl(solar_gpu_context* c, const solar_gpu_options* o_in, const so
     c->have_barle = !c->have_csr;
     c->csr_total = c->have_csr ? l->data_size : 0;
     c->barle_total = c->have_barle ? l->data_size : 0;
-    RK(ensure(c->shadow, sizeof(uint32_t) * (size_t)N * words32));
+    RK(ensure(c, c->shadow, sizeof(uint32_t) * (size_t)N * words32));
     CK(cudaMemcpyAsync(c->shadow.p, l->shadow, sizeof(uint32_t) * (size_t)N * words32, cudaMemcpyHostToDevice, st));
     DevBuf& off = c->have_csr ? c->csr_off : c->barle_off;
     DevBuf& dat = c->have_csr ? c->csr_ids : c->barle_bytes;
     const size_t dbytes = (size_t)l->data_size * (c->have_csr ? sizeof(int) : 1);
-    RK(ensure(off, sizeof(long long) * ((size_t)N + 1)));
-    RK(ensure(dat, dbytes ? dbytes : 16));
+    RK(ensure(c, off, sizeof(long long) * ((size_t)N + 1)));
+    RK(ensure(c, dat, dbytes ? dbytes : 16));
     CK(cudaMemcpyAsync(off.p, l->offsets, sizeof(long long) * ((size_t)N + 1), cudaMemcpyHostToDevice, st));
     if (dbytes) CK(cudaMemcpyAsync(dat.p, l->data, dbytes, cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(c->ev[2], st));
@@ -815,11 +852,11 @@ int trace_subset_impl(solar_gpu_context* c, const solar_gpu_scene* s, const int*
     if (words_out) *words_out = words32;
     if (n == 0) return SOLAR_GPU_OK;
     // the listed voxels must exist (the tracer reads their parents)
-    RK(ensure(c->err, sizeof(int)));
-    RK(ensure(c->shadow, sizeof(uint32_t) * (size_t)N * words32));
+    RK(ensure(c, c->err, sizeof(int)));
+    RK(ensure(c, c->shadow, sizeof(uint32_t) * (size_t)N * words32));
     CK(cudaMemsetAsync(c->shadow.p, 0, sizeof(uint32_t) * (size_t)N * words32, st));
-    RK(ensure(c->raw, sizeof(int) * (size_t)n * D));
-    RK(ensure(c->order_inv, sizeof(int) * (size_t)n));
+    RK(ensure(c, c->raw, sizeof(int) * (size_t)n * D));
+    RK(ensure(c, c->order_inv, sizeof(int) * (size_t)n));
     k_check_ids<<<(n + 255) / 256, 256, 0, st>>>(voxels, n, N, as<int>(c->err));
     CK(cudaMemcpyAsync(c->h_scalars, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -908,7 +945,6 @@ int solar_gpu_create(int device, solar_gpu_context** out)
     return SOLAR_GPU_OK;
 }
 
-static constexpr int kNumBufs = 65;
 
 static void all_bufs(solar_gpu_context* c, DevBuf** out)
 {
@@ -925,6 +961,19 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
+}
+
+int solar_gpu_set_memory_limit(solar_gpu_context* c, long long bytes)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    if (bytes < 0) return fail(SOLAR_GPU_ERR_ARG, "memory limit must be >= 0");
+    c->mem_limit = bytes;
+    return SOLAR_GPU_OK;
+}
+
+long long solar_gpu_memory_held(solar_gpu_context* c)
+{
+    return c ? (long long)held_bytes(c) : 0;
 }
 
 int solar_gpu_release(solar_gpu_context* c)
@@ -993,12 +1042,12 @@ int solar_gpu_run_host(solar_gpu_context* c, const solar_gpu_options* o, const s
     CK(cudaSetDevice(c->device));
     cudaStream_t st = c->own;
     const size_t N = (size_t)s->num_total_voxels, T = (size_t)s->num_top_voxels, NW = N - T;
-    RK(ensure(c->in_grid, sizeof(float) * T));
-    RK(ensure(c->in_pp, sizeof(int) * N));
-    RK(ensure(c->in_wz, sizeof(float) * (NW ? NW : 1)));
-    RK(ensure(c->in_slopes, sizeof(float) * N));
-    RK(ensure(c->in_aspects, sizeof(float) * N));
-    RK(ensure(c->out_f32, sizeof(float) * N));
+    RK(ensure(c, c->in_grid, sizeof(float) * T));
+    RK(ensure(c, c->in_pp, sizeof(int) * N));
+    RK(ensure(c, c->in_wz, sizeof(float) * (NW ? NW : 1)));
+    RK(ensure(c, c->in_slopes, sizeof(float) * N));
+    RK(ensure(c, c->in_aspects, sizeof(float) * N));
+    RK(ensure(c, c->out_f32, sizeof(float) * N));
     CK(cudaMemcpyAsync(c->in_grid.p, s->grid, sizeof(float) * T, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->in_pp.p, s->pixel_parent, sizeof(int) * N, cudaMemcpyHostToDevice, st));
     if (NW) CK(cudaMemcpyAsync(c->in_wz.p, s->wall_z, sizeof(float) * NW, cudaMemcpyHostToDevice, st));

@@ -194,10 +194,11 @@ cudaError_t launch_tile_layout(int pass, int NG, int R, const int* start, const 
                                const unsigned short* slots, const float* wts, int* gcnt, int* gnch,
                                const long long* gbase, const long long* tbase, int* table,
                                unsigned short* erow, float4* ew, cudaStream_t st);
-// BF16 tensor-core GEMM (surrogate.cu): C = A x B^T (+bias, ReLU); M, N
-// multiples of 128, K of 64; C and/or Cb (bf16 copy) may be null.
+// BF16 tensor-core GEMM (surrogate.cu): C = A x B^T (+bias, ReLU); M a
+// multiple of 128, N and K of 64; C and/or Cb (bf16 copy) may be null.
+// stall != 0 withholds the operand loads (self-test of the bounded waits).
 cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, const float* bias, int M, int N,
-                             int K, int relu, int* err, cudaStream_t st);
+                             int K, int relu, int* err, cudaStream_t st, int stall = 0);
 // slab: [N][B] rows of every voxel (neighbor values and each voxel's own term).
 cudaError_t launch_reflect_tile(int B, const float* slab, const TileLists& tl, const int* order, const Accum& acc,
                                 int* err, cudaStream_t st);

@@ -60,7 +60,8 @@ __device__ __forceinline__ unsigned long long g_ns()
     return t;
 }
 
-__device__ __forceinline__ bool wait_parity(unsigned bar, unsigned parity, const volatile int* fail)
+__device__ __forceinline__ bool wait_parity(unsigned bar, unsigned parity, const volatile int* fail,
+                                            unsigned long long limit_ns = kGemmWaitNs)
 {
     unsigned long long t0 = 0;
     for (unsigned i = 0;; ++i) {
@@ -77,7 +78,7 @@ __device__ __forceinline__ bool wait_parity(unsigned bar, unsigned parity, const
             if (fail && *fail) return false;
             const unsigned long long t = g_ns();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > kGemmWaitNs) return false;
+            else if (t - t0 > limit_ns) return false;
         }
     }
 }
@@ -102,7 +103,7 @@ template <int BN>
 __global__ void __launch_bounds__(kGemmThreads, 1)
 k_gemm_bf16(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
             float* __restrict__ C, __nv_bfloat16* __restrict__ Cb, const float* __restrict__ bias, int M, int N, int K,
-            int relu, int* __restrict__ err)
+            int relu, int* __restrict__ err, int stall)
 {
     extern __shared__ __align__(1024) unsigned char gsm[];
     __shared__ __align__(8) unsigned long long full[kGemmStages], empty[kGemmStages], done;
@@ -136,8 +137,9 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
     int issued = 0;   // producer: stages loaded
     if (threadIdx.x == 0) {
-        // ---- producer
-        for (int k = 0; k < nk; ++k) {
+        // ---- producer (stall: issues nothing, so the MMA thread's bounded
+        // wait runs out; the self-test of the error path)
+        for (int k = 0; k < (stall ? 0 : nk); ++k) {
             const int s = k % kGemmStages;
             if (k >= kGemmStages &&
                 !wait_parity(s_u32(&empty[s]), (unsigned)(((k / kGemmStages) - 1) & 1), &s_fail)) {
@@ -183,7 +185,8 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
                      ::"r"(s_u32(&done)) : "memory");
     }
     // everyone: the accumulator is ready (or the run failed)
-    if (!wait_parity(s_u32(&done), 0u, nullptr)) s_fail = 1;
+    // longer than the pipeline's waits, so a failed pipeline always signals first
+    if (!wait_parity(s_u32(&done), 0u, nullptr, 2 * kGemmWaitNs)) s_fail = 1;
     __syncthreads();
     const bool ok = !s_fail;   // uniform over the CTA
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -564,7 +567,7 @@ bool make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows)
 
 template <int BN>
 cudaError_t launch_gemm_tiles(const void* A, const void* B, float* C, void* Cb, const float* bias, int M, int N,
-                              int K, int relu, int* err, cudaStream_t st)
+                              int K, int relu, int* err, cudaStream_t st, int stall)
 {
     CUtensorMap mapA, mapB;
     if (!make_map(&mapA, A, M, K, kTm) || !make_map(&mapB, B, N, K, BN)) return cudaErrorInvalidValue;
@@ -580,7 +583,7 @@ cudaError_t launch_gemm_tiles(const void* A, const void* B, float* C, void* Cb, 
     }
     const dim3 grid(N / BN, M / kTm);
     k_gemm_bf16<BN><<<grid, kGemmThreads, GemmShape<BN>::kSmem, st>>>(
-        mapA, mapB, C, static_cast<__nv_bfloat16*>(Cb), bias, M, N, K, relu, err);
+        mapA, mapB, C, static_cast<__nv_bfloat16*>(Cb), bias, M, N, K, relu, err, stall);
     return cudaGetLastError();
 }
 }  // namespace
@@ -589,7 +592,7 @@ cudaError_t launch_gemm_tiles(const void* A, const void* B, float* C, void* Cb, 
 // SMs (148 on B200) at least once, 64 when N is not a multiple of 128,
 // else 128.  SGB_GEMM_BN (64, 128, 256) forces a width that divides N.
 cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, const float* bias, int M, int N,
-                             int K, int relu, int* err, cudaStream_t st)
+                             int K, int relu, int* err, cudaStream_t st, int stall)
 {
     if (M <= 0 || N <= 0 || K <= 0 || M % kTm || N % 64 || K % kTk) return cudaErrorInvalidValue;
     int bn = N % 128 ? 64 : (N % 256 == 0 && (long long)(M / kTm) * (N / 256) >= 148) ? 256 : 128;
@@ -598,9 +601,9 @@ cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, c
         if ((f == 64 || f == 128 || f == 256) && N % f == 0) bn = f;
     }
     switch (bn) {
-    case 256: return launch_gemm_tiles<256>(A, B, C, Cb, bias, M, N, K, relu, err, st);
-    case 128: return launch_gemm_tiles<128>(A, B, C, Cb, bias, M, N, K, relu, err, st);
-    default: return launch_gemm_tiles<64>(A, B, C, Cb, bias, M, N, K, relu, err, st);
+    case 256: return launch_gemm_tiles<256>(A, B, C, Cb, bias, M, N, K, relu, err, st, stall);
+    case 128: return launch_gemm_tiles<128>(A, B, C, Cb, bias, M, N, K, relu, err, st, stall);
+    default: return launch_gemm_tiles<64>(A, B, C, Cb, bias, M, N, K, relu, err, st, stall);
     }
 }
 
@@ -767,21 +770,22 @@ int solar_gpu_sg_transpose_f32(const float* in, int R, int C, float* out, void* 
     return sg_status(cudaSuccess);
 }
 
-int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N,
-                        int K, int relu, void* stream)
+namespace {
+int gemm_call(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N, int K, int relu,
+              cudaStream_t st, int stall)
 {
     if (!A || !B || (!C && !C_bf16) || ((uintptr_t)A | (uintptr_t)B | (uintptr_t)C | (uintptr_t)C_bf16) % 16) {
         sgb::set_last_error("gemm: null or misaligned (16-byte) pointers");
         return -1;
     }
     int* err = nullptr;
-    cudaError_t e = cudaMallocAsync(&err, sizeof(int), (cudaStream_t)stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), (cudaStream_t)stream);
-    if (e == cudaSuccess) e = sgb::launch_gemm_bf16(A, B, C, C_bf16, bias, M, N, K, relu, err, (cudaStream_t)stream);
+    cudaError_t e = cudaMallocAsync(&err, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = sgb::launch_gemm_bf16(A, B, C, C_bf16, bias, M, N, K, relu, err, st, stall);
     int flag = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
-    if (err) cudaFreeAsync(err, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (err) cudaFreeAsync(err, st);
     if (e != cudaSuccess) {
         sgb::set_last_error(cudaGetErrorString(e));
         return e == cudaErrorInvalidValue ? -1 : -2;
@@ -791,6 +795,36 @@ int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, co
         return -5;
     }
     return 0;
+}
+}  // namespace
+
+int solar_gpu_gemm_bf16(const void* A, const void* B, float* C, void* C_bf16, const float* bias, int M, int N,
+                        int K, int relu, void* stream)
+{
+    return gemm_call(A, B, C, C_bf16, bias, M, N, K, relu, (cudaStream_t)stream, 0);
+}
+
+int solar_gpu_selftest_bounded_wait(void* stream)
+{
+    // One 128 x 64 x 64 tile whose operand loads are never issued: the MMA
+    // thread's wait for them runs out after about a second, the kernel flags
+    // the error, frees its TMEM and exits; the call reports it like any
+    // expired wait.
+    cudaStream_t st = (cudaStream_t)stream;
+    void* buf = nullptr;
+    const size_t a_bytes = 128 * 64 * 2, b_bytes = 64 * 64 * 2, c_bytes = 128 * 64 * 4;
+    cudaError_t e = cudaMallocAsync(&buf, a_bytes + b_bytes + c_bytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(buf, 0, a_bytes + b_bytes + c_bytes, st);
+    if (e != cudaSuccess) {
+        sgb::set_last_error(cudaGetErrorString(e));
+        return -2;
+    }
+    char* p = static_cast<char*>(buf);
+    const int rc = gemm_call(p, p + a_bytes, reinterpret_cast<float*>(p + a_bytes + b_bytes), nullptr, nullptr, 128,
+                             64, 64, 0, st, 1);
+    cudaFreeAsync(buf, st);
+    cudaStreamSynchronize(st);
+    return rc;
 }
 
 }  // extern "C"
