@@ -109,6 +109,20 @@ def trace(scene, bins: dict | None = None, v0: int = 0, v1: int | None = None,
     return off, out.astype(np.int32), sh
 
 
+def trace_one(grid: np.ndarray, maxz: float, gx: int, gy: int, base_z: float, c, is_upper: bool,
+              fma_mode: int = 1) -> int:
+    """One DDA ray over a bare heightmap grid [H][W] from cell (gx, gy) at
+    base_z along c = (cx, cy, cz); the 1-based hit cell id or 0."""
+    g = np.ascontiguousarray(grid, np.float32)
+    H, W = g.shape
+    f = lib().orc_trace_one
+    f.restype = C.c_int
+    f.argtypes = [_P, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                  C.c_int, C.c_int]
+    return f(_ptr(g), W, H, float(maxz), int(gx), int(gy), float(base_z), float(np.float32(c[0])),
+             float(np.float32(c[1])), float(np.float32(c[2])), int(bool(is_upper)), int(fma_mode))
+
+
 # ---------------------------------------------------------------- ba-RLE
 
 def barle_encode(ids) -> bytes:

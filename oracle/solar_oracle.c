@@ -133,13 +133,12 @@ typedef struct {
     int fma_mode;
 } orc_scene;
 
-/* Traces one ray; returns the 1-based hit cell id or 0. */
-static int trace_ray(const orc_scene* s, int t_id, float cx, float cy, float cz, int is_upper)
+/* Traces one ray from cell (gx, gy) at height base_z (the origin is the
+   cell corner plus 2 * Cdir, viewshed_kernels.cu:27-29); returns the
+   1-based hit cell id or 0. */
+static int trace_ray_from(const orc_scene* s, int gx, int gy, float base_z, float cx, float cy, float cz,
+                          int is_upper)
 {
-    int top_id = s->pix_parent[t_id];
-    int gx = top_id % s->W;
-    int gy = top_id / s->W;
-    float base_z = (t_id < s->num_top) ? s->grid[gx + gy * s->W] : s->wall_z[t_id - s->num_top];
     /* Cdir * 2 is exact, so fused or not these three match. */
     float ox = (float)gx + cx * 2.0f;
     float oy = (float)gy + cy * 2.0f;
@@ -161,6 +160,31 @@ static int trace_ray(const orc_scene* s, int t_id, float cx, float cy, float cz,
         if (!is_upper && zr < 0.0f) return 0;
         if (s->grid[ix + iy * s->W] - zr > 0.01f) return ix + iy * s->W + 1;
     }
+}
+
+/* Traces one ray of voxel t_id (viewshed_kernels.cu:15-25: a wall voxel
+   starts at its parent column at wall_z). */
+static int trace_ray(const orc_scene* s, int t_id, float cx, float cy, float cz, int is_upper)
+{
+    int top_id = s->pix_parent[t_id];
+    int gx = top_id % s->W;
+    int gy = top_id / s->W;
+    float base_z = (t_id < s->num_top) ? s->grid[gx + gy * s->W] : s->wall_z[t_id - s->num_top];
+    return trace_ray_from(s, gx, gy, base_z, cx, cy, cz, is_upper);
+}
+
+/* One ray over a bare heightmap (known-answer tests of the DDA). */
+int orc_trace_one(const float* grid, int W, int H, float maxz, int gx, int gy, float base_z, float cx, float cy,
+                  float cz, int is_upper, int fma_mode)
+{
+    orc_scene s;
+    memset(&s, 0, sizeof s);
+    s.grid = grid;
+    s.W = W;
+    s.H = H;
+    s.maxz = maxz;
+    s.fma_mode = fma_mode;
+    return trace_ray_from(&s, gx, gy, base_z, cx, cy, cz, is_upper);
 }
 
 /* Per-voxel open-addressing set with generation stamps (dedupe helper). */

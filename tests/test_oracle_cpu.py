@@ -188,3 +188,75 @@ def test_lists_cache_roundtrip_and_fingerprints(tmp_path):
     cache.save_lists(p, rb, s)
     gb = cache.load_lists(p)
     assert np.array_equal(gb["barle"], bbytes) and "csr_off" not in gb
+
+
+# ---- DDA known answers on hand-made heightmaps (viewshed_kernels.cu:7-59) --------------------
+# Answers worked out by hand from the ray geometry: origin = cell corner + 2 * Cdir, the start
+# cell is never tested, a hit is height - z_ray > 0.01 at the cell entered, an upward ray stops
+# above the maximum height, a downward one below 0, and a tie tMaxX == tMaxY steps y.
+
+def _dir(az_deg: float, el_deg: float):
+    """(cx, cy, cz) for azimuth/elevation in the reference's convention: x = cos e sin az,
+    y = -cos e cos az, z = sin e."""
+    a, e = np.radians(az_deg), np.radians(el_deg)
+    return (np.float32(np.cos(e) * np.sin(a)), np.float32(-np.cos(e) * np.cos(a)), np.float32(np.sin(e)))
+
+
+def _grid(towers=()):
+    g = np.zeros((16, 16), np.float32)
+    for x, y, h in towers:
+        g[y, x] = h
+    return g
+
+
+def test_dda_flat_plane_has_no_hits():
+    from oracle import oracle as O
+    g = _grid()
+    for az in np.arange(2.5, 360.0, 5.0):
+        for el in np.arange(-87.5, 90.0, 5.0):
+            for gx, gy in ((0, 0), (7, 9), (15, 15)):
+                assert O.trace_one(g, 0.0, gx, gy, 0.0, _dir(az, el), el > 0) == 0
+
+
+def test_dda_single_tower():
+    from oracle import oracle as O
+    g = _grid([(10, 5, 10.0)])
+    east = lambda el: (np.float32(np.cos(np.radians(el))), np.float32(0.0), np.float32(np.sin(np.radians(el))))
+    # at 60 degrees the ray is 8.66 m high entering x = 10: hit (id 10 + 5 * 16 + 1)
+    assert O.trace_one(g, 10.0, 5, 5, 0.0, east(60.0), True) == 91
+    # at 70 degrees it passes 10 m (the maximum height) over x = 9 and stops
+    assert O.trace_one(g, 10.0, 5, 5, 0.0, east(70.0), True) == 0
+    # westward there is nothing to hit before the grid edge
+    west = (np.float32(-np.cos(np.radians(10.0))), np.float32(0.0), np.float32(np.sin(np.radians(10.0))))
+    assert O.trace_one(g, 10.0, 5, 5, 0.0, west, True) == 0
+    # from the tower top downward to the west: the ray goes below 0 before anything is higher
+    down = (np.float32(-np.cos(np.radians(30.0))), np.float32(0.0), np.float32(-0.5))
+    assert O.trace_one(g, 10.0, 10, 5, 10.0, down, False) == 0
+
+
+def test_dda_start_cell_is_not_tested():
+    from oracle import oracle as O
+    c = (np.float32(np.cos(np.radians(10.0))), np.float32(0.0), np.float32(np.sin(np.radians(10.0))))
+    # origin x = 5 + 2 cos(10 deg) = 6.97: the start cell is (6, 5); a tower there is skipped
+    assert O.trace_one(_grid([(6, 5, 10.0)]), 10.0, 5, 5, 0.0, c, True) == 0
+    assert O.trace_one(_grid([(7, 5, 10.0)]), 10.0, 5, 5, 0.0, c, True) == 7 + 5 * 16 + 1
+
+
+def test_dda_grid_edge():
+    from oracle import oracle as O
+    # along the last column toward -y: start cell (15, 13), the first cell entered is (15, 12)
+    c = (np.float32(0.0), np.float32(-np.cos(np.radians(10.0))), np.float32(np.sin(np.radians(10.0))))
+    assert O.trace_one(_grid([(15, 12, 10.0)]), 10.0, 15, 15, 0.0, c, True) == 15 + 12 * 16 + 1
+    # from the corner outward: the first step leaves the grid
+    out = (np.float32(-0.6), np.float32(-0.6), np.float32(0.5291503))
+    assert O.trace_one(_grid([(0, 0, 10.0)]), 10.0, 0, 0, 0.0, out, True) == 0
+
+
+def test_dda_tie_steps_y_first():
+    from oracle import oracle as O
+    # cx == cy: from origin (6.41, 6.41) tMaxX == tMaxY exactly, and the tie steps y into (6, 7)
+    c = (np.float32(0.7066), np.float32(0.7066), np.float32(0.0349))
+    assert O.trace_one(_grid([(6, 7, 10.0)]), 10.0, 5, 5, 0.0, c, True) == 6 + 7 * 16 + 1
+    # stepping y first, the ray never enters (7, 6): it goes (6, 7), (7, 7), (7, 8), ...
+    assert O.trace_one(_grid([(7, 6, 10.0)]), 10.0, 5, 5, 0.0, c, True) == 0
+    assert O.trace_one(_grid([(7, 7, 10.0)]), 10.0, 5, 5, 0.0, c, True) == 7 + 7 * 16 + 1
