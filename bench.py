@@ -31,6 +31,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "annual voxel-hours/s on 1 B200 vs plain per-hour path at ≤1e-4 rel err"
 UNIT = "voxel-hours/s"
+N_DIRS = 2592      # traced directions per voxel: 72 azimuth x 36 elevation bins of 5 degrees
 FMT_NAMES = {0: "CSR", 1: "ba-RLE"}
 ACC_NAMES = {0: "fp32 block sums + fp64 annual", 1: "kahan-compensated fp32", 2: "plain fp32"}
 
@@ -427,6 +428,7 @@ def run_ours(args, world, rank, local, pg):
         extra["error_vs_fp64"] = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),
                                   "oracle": "FP64 annual-sum form on the GPU-built neighbor lists and shadow bits"}
     cpu = None
+    steps_per_ray = nst = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle as O
         rng = np.random.default_rng(0)
@@ -438,6 +440,9 @@ def run_ours(args, world, rank, local, pg):
                           f"top-cell solar table for one {r['hblock']}-hour block ({r['table_s']:.2f} s), "
                           f"per-hour reflection sums of the {ns} voxels for that block ({r['sums_s']:.2f} s); "
                           f"scaled to {N} voxels x {r['hours']} h")}
+        # the workload's mean DDA steps per ray, counted by the oracle on a sample
+        nst = min(ns, 2000)
+        steps_per_ray = float(O.trace_steps(scene, smp[:nst]).astype(np.float64).mean())
 
     if rank == 0:
         line = {
@@ -452,6 +457,16 @@ def run_ours(args, world, rank, local, pg):
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
             "stage_ms": {g: round(v[0] / args.steps, 3) for g, v in ktimes.items()},
         }
+        if "trace" in ktimes:
+            # Stage 1 in its own units: rays = voxels x 2592 directions per run
+            t_trace = ktimes["trace"][0] / args.steps / 1e3
+            rays = float(N) * N_DIRS
+            st1 = {"rays_per_run": rays, "rays_per_s": rays / t_trace, "trace_ms": round(t_trace * 1e3, 3)}
+            if steps_per_ray is not None:
+                st1.update({"dda_steps_per_ray": round(steps_per_ray, 3),
+                            "dda_steps_per_s": steps_per_ray * rays / t_trace,
+                            "steps_source": f"mean DDA steps per ray counted by the oracle on {nst} random voxels"})
+            line["stage1"] = st1
         line.update(extra)
         print(json.dumps(line), flush=True)
     ctx.close()

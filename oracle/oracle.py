@@ -123,6 +123,23 @@ def trace_one(grid: np.ndarray, maxz: float, gx: int, gy: int, base_z: float, c,
              float(np.float32(c[1])), float(np.float32(c[2])), int(bool(is_upper)), int(fma_mode))
 
 
+def trace_steps(scene, voxels: np.ndarray, bins: dict | None = None) -> np.ndarray:
+    """DDA steps of every ray of the listed voxels: int16 [n][D] (saturating
+    at 32767); a step is one move to the next cell (the loop of
+    viewshed_kernels.cu:31-58)."""
+    if bins is None:
+        bins = sky_bins(scene.sun)
+    dirs, dense, upper = directions(bins)
+    vox = np.ascontiguousarray(voxels, np.int32)
+    D = dirs.shape[0]
+    steps = np.zeros((vox.size, D), np.int16)
+    wall = scene.wall_z if scene.wall_z.size else np.zeros(1, np.float32)
+    lib().orc_trace_steps(_ptr(scene.grid), scene.width, scene.height, scene.num_total, scene.num_top,
+                          _ptr(scene.pixel_parent), _ptr(wall), C.c_float(scene.max_height), _ptr(dirs),
+                          _ptr(dense), _ptr(upper), D, _ptr(vox), vox.size, steps.ctypes.data_as(_P))
+    return steps
+
+
 # ---------------------------------------------------------------- ba-RLE
 
 def barle_encode(ids) -> bytes:
