@@ -29,8 +29,9 @@ constexpr int kDedupeWarps = 4;
 constexpr int kHashSlots = 4096;   // > 2592 possible distinct hits per voxel
 constexpr int kDedupeBatch = 9;    // 2592 = 9 batches of 9 rounds of 32 directions
 
-__device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, int H, float maxz,
-                                         int gx, int gy, float base_z, const DirEntry& d)
+template <bool UP>
+__device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, int H, float maxz, int gx, int gy,
+                                         float base_z, const DirEntry& d)
 {
     // Cdir * 2.0f is exact, so these match the reference fused or not.
     const float ox = __fadd_rn((float)gx, __fmul_rn(d.cx, 2.0f));
@@ -44,18 +45,30 @@ __device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, 
     float tMaxY = __fdiv_rn(py ? __fsub_rn(__fadd_rn((float)iy, 1.0f), oy) : __fsub_rn(oy, (float)iy), d.ay);
     const int sx = px ? 1 : -1;
     const int sy = py ? 1 : -1;
-    const bool up = (d.meta >> 16) & 1;
-    // Each step moves ix or iy one cell in a fixed direction, so the loop
-    // leaves the grid after at most W + H steps.
+    // The first step checks both coordinates (the start cell, never tested,
+    // may lie outside the grid); after it the ray is inside, and each later
+    // step checks only the coordinate it moves, by counting the steps left
+    // on that axis.  Each step moves one cell in a fixed direction, so the
+    // loop leaves the grid after at most W + H steps.
+    float t;
+    if (tMaxX < tMaxY) { t = tMaxX; ix += sx; tMaxX = __fadd_rn(tMaxX, d.dX); }
+    else               { t = tMaxY; iy += sy; tMaxY = __fadd_rn(tMaxY, d.dY); }
+    if ((unsigned)ix >= (unsigned)W || (unsigned)iy >= (unsigned)H) return 0;
+    int left_x = px ? W - 1 - ix : ix;
+    int left_y = py ? H - 1 - iy : iy;
+    const int step_y = py ? W : -W;
+    int cell = ix + iy * W;
     for (;;) {
-        float t;
-        if (tMaxX < tMaxY) { t = tMaxX; ix += sx; tMaxX = __fadd_rn(tMaxX, d.dX); }
-        else               { t = tMaxY; iy += sy; tMaxY = __fadd_rn(tMaxY, d.dY); }
-        if ((unsigned)ix >= (unsigned)W || (unsigned)iy >= (unsigned)H) return 0;
         const float zr = __fmaf_rn(d.cz, t, oz);
-        if (up ? (zr > maxz) : (zr < 0.0f)) return 0;
-        const int cell = ix + iy * W;
+        if (UP ? (zr > maxz) : (zr < 0.0f)) return 0;
         if (__fsub_rn(__ldg(grid + cell), zr) > 0.01f) return cell + 1;
+        if (tMaxX < tMaxY) {
+            if (--left_x < 0) return 0;
+            t = tMaxX; cell += sx; tMaxX = __fadd_rn(tMaxX, d.dX);
+        } else {
+            if (--left_y < 0) return 0;
+            t = tMaxY; cell += step_y; tMaxY = __fadd_rn(tMaxY, d.dY);
+        }
     }
 }
 
@@ -85,7 +98,10 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
     for (int g0 = gb * kRawGroup; g0 < ge * kRawGroup; g0 += kRawGroup) {
         for (int k = 0; k < kRawGroup; ++k) {
             const DirEntry d = dirs[g0 + k];
-            const int hit = active ? trace_ray(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d) : 0;
+            // up/down is the same for the whole warp (one direction at a time)
+            const int hit = !active ? 0
+                            : ((d.meta >> 16) & 1) ? trace_ray<true>(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d)
+                                                   : trace_ray<false>(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d);
             stage[k][threadIdx.x] = hit;
             const int dense = (d.meta & 0xFFFF) - 1;   // warp-uniform
             if (dense >= 0) {
