@@ -93,6 +93,7 @@ struct solar_gpu_context {
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
+    size_t dev_total = 0;       // device memory size, read once at creation
     // last Stage 1 result
     int N = 0, T = 0, words32 = 0, active = 0;
     long long csr_total = 0, barle_total = 0;
@@ -328,6 +329,10 @@ int prepare(solar_gpu_context* c, const solar_gpu_scene* s, SkyTables& sky, cuda
 
 long long auto_chunk(solar_gpu_context* c, int N, int D)
 {
+    // A raw buffer kept from an earlier call that holds the whole scene is
+    // reused without asking the driver for free memory (that query can wait
+    // behind other processes' driver calls, e.g. monitoring tools).
+    if (c->raw.cap >= sizeof(int) * (size_t)N * D) return N;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
     if (c->mem_limit > 0) {
@@ -456,9 +461,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     // A raw hit buffer above a quarter of the device (scenes of tens of
     // millions of voxels) is released here to leave room for Stage 2/3;
     // smaller ones are kept for the next call.
-    size_t fr = 0, tot = 0;
-    CK(cudaMemGetInfo(&fr, &tot));
-    if (c->raw.cap > tot / 4) {
+    if (c->raw.cap > c->dev_total / 4) {
         CK(cudaFree(c->raw.p));
         c->raw.p = nullptr;
         c->raw.cap = 0;
@@ -633,9 +636,7 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 // Per-voxel weights and slots are dead now; above 1/16 of the
                 // device (scenes of tens of millions of voxels) they are
                 // released to make room for the slab.
-                size_t fr = 0, tot = 0;
-                CK(cudaMemGetInfo(&fr, &tot));
-                if (c->w_val.cap + c->tile_slot.cap > tot / 16) {
+                if (c->w_val.cap + c->tile_slot.cap > c->dev_total / 16) {
                     CK(cudaFree(c->w_val.p));
                     CK(cudaFree(c->tile_slot.p));
                     c->w_val.p = c->tile_slot.p = nullptr;
@@ -940,6 +941,8 @@ int solar_gpu_create(int device, solar_gpu_context** out)
     cudaError_t e1 = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
     for (int i = 0; i < 4 && e1 == cudaSuccess; ++i) e1 = cudaEventCreate(&c->ev[i]);
     if (e1 == cudaSuccess) e1 = cudaMallocHost((void**)&c->h_scalars, 64);
+    size_t free_b = 0;
+    if (e1 == cudaSuccess) e1 = cudaMemGetInfo(&free_b, &c->dev_total);
     if (e1 != cudaSuccess) { solar_gpu_destroy(c); return cuda_fail(e1, "context setup", __LINE__); }
     *out = c;
     return SOLAR_GPU_OK;
