@@ -233,6 +233,191 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
 }
 
+// Persistent form for grids of more than one wave: one CTA per SM walks the
+// tiles blockIdx.x, blockIdx.x + gridDim.x, ... with 6 warps:
+//   * warp 0 (one thread) loads the shared-memory ring by TMA, its stage
+//     counter running on across tiles;
+//   * warp 1 allocates two accumulators of BN TMEM columns and one thread
+//     issues the MMAs of tile i into accumulator i % 2, then commits to that
+//     accumulator's full barrier;
+//   * warps 2..5 are the epilogue: warp w reads TMEM lanes 32 (w % 4) ..
+//     (rows of the tile), stores them and arrives on the accumulator's empty
+//     barrier, so tile i's epilogue overlaps tile i + 1's MMAs.
+// Every wait is bounded and checks a shared failure flag, so all roles leave
+// their loops once one wait runs out; a last commit lets the MMAs in flight
+// finish and the TMA thread waits for its copies before TMEM is freed.
+constexpr int kPersThreads = 192;
+
+template <int BN>
+__global__ void __launch_bounds__(kPersThreads, 1)
+k_gemm_bf16_pers(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                 float* __restrict__ C, __nv_bfloat16* __restrict__ Cb, const float* __restrict__ bias, int M, int N,
+                 int K, int relu, int* __restrict__ err)
+{
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    __shared__ __align__(8) unsigned long long full[kGemmStages], empty[kGemmStages], tfull[2], tempty[2], done;
+    __shared__ unsigned tmem_base;
+    __shared__ volatile int s_fail;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    using S = GemmShape<BN>;
+    const unsigned base = (s_u32(gsm) + 1023u) & ~1023u;
+    const int nk = K / kTk;
+    const int ntn = N / BN;
+    const int ntiles = (M / kTm) * ntn;
+    const int my_tiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_u32(&tmem_base)),
+                     "r"(2 * BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kGemmStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&full[s])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&empty[s])), "r"(1));
+        }
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&tfull[b])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&tempty[b])), "r"(4));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_u32(&done)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = tmem_base;
+
+    long long issued = 0;   // TMA thread: stages loaded
+    if (threadIdx.x == 0) {
+        // ---- TMA
+        long long g = 0;
+        for (int i = 0; i < my_tiles && !s_fail; ++i) {
+            const int t = (int)blockIdx.x + i * (int)gridDim.x;
+            const int m0 = (t / ntn) * kTm, n0 = (t % ntn) * BN;
+            for (int k = 0; k < nk; ++k, ++g) {
+                const int s = (int)(g % kGemmStages);
+                if (g >= kGemmStages &&
+                    !wait_parity(s_u32(&empty[s]), (unsigned)(((g / kGemmStages) - 1) & 1), &s_fail)) {
+                    s_fail = 1;
+                    break;
+                }
+                const unsigned sa = base + (unsigned)(s * S::kStage), sb = sa + S::kStageA;
+                const unsigned fb = s_u32(&full[s]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                             "r"((unsigned)S::kStage) : "memory");
+                tma_box(sa, &mapA, k * kTk, m0, fb);
+                tma_box(sb, &mapB, k * kTk, n0, fb);
+                ++issued;
+            }
+        }
+    } else if (threadIdx.x == 32) {
+        // ---- MMA
+        long long g = 0;
+        for (int i = 0; i < my_tiles; ++i) {
+            const int b = i & 1;
+            if (i >= 2 && !wait_parity(s_u32(&tempty[b]), (unsigned)(((i >> 1) - 1) & 1), &s_fail)) {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned acc_cols = tmem + (unsigned)(b * BN);
+            bool bad = false;
+            for (int k = 0; k < nk; ++k, ++g) {
+                const int s = (int)(g % kGemmStages);
+                if (!wait_parity(s_u32(&full[s]), (unsigned)((g / kGemmStages) & 1), &s_fail)) {
+                    bad = true;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const unsigned sa = base + (unsigned)(s * S::kStage), sb = sa + S::kStageA;
+#pragma unroll
+                for (int j = 0; j < kTk / 16; ++j) {
+                    const unsigned long long da = smem_desc_sw128(sa + 32u * j);
+                    const unsigned long long db = smem_desc_sw128(sb + 32u * j);
+                    const unsigned acc = (k > 0 || j > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                        ::"r"(acc_cols), "l"(da), "l"(db), "r"(S::kIdesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                             ::"r"(s_u32(&empty[s])) : "memory");
+            }
+            if (bad) {
+                s_fail = 1;
+                break;
+            }
+            // accumulator b holds tile i once these MMAs complete
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(s_u32(&tfull[b])) : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(s_u32(&done)) : "memory");
+    } else if (warp >= 2) {
+        // ---- epilogue: this warp's TMEM lanes are rows 32q .. 32q + 31 of the tile
+        const int q = warp & 3;
+        for (int i = 0; i < my_tiles; ++i) {
+            const int b = i & 1;
+            if (!wait_parity(s_u32(&tfull[b]), (unsigned)((i >> 1) & 1), &s_fail)) {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int t = (int)blockIdx.x + i * (int)gridDim.x;
+            const int m0 = (t / ntn) * kTm, n0 = (t % ntn) * BN;
+            const int row = m0 + 32 * q + lane;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 8) {
+                unsigned r[8];
+                const unsigned taddr = tmem + ((unsigned)(32 * q) << 16) + (unsigned)(b * BN + c0);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                               "=r"(r[7])
+                             : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    v[j] = __uint_as_float(r[j]) + (bias ? bias[n0 + c0 + j] : 0.0f);
+                    if (relu) v[j] = fmaxf(v[j], 0.0f);
+                }
+                if (C) {
+                    float4* dst = reinterpret_cast<float4*>(C + (size_t)row * N + n0 + c0);
+                    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+                    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+                }
+                if (Cb) {
+                    __nv_bfloat162 h[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                    *reinterpret_cast<uint4*>(Cb + (size_t)row * N + n0 + c0) = *reinterpret_cast<uint4*>(h);
+                }
+            }
+            // the accumulator may be overwritten once all four warps have read it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(s_u32(&tempty[b])) : "memory");
+        }
+    }
+    // every MMA issued has completed (or the wait gave up after twice the pipeline's limit)
+    if (!wait_parity(s_u32(&done), 0u, nullptr, 2 * kGemmWaitNs)) s_fail = 1;
+    __syncthreads();
+    if (s_fail && threadIdx.x == 0) {
+        atomicOr(err, kErrWaitTimeout);
+        // let this thread's TMA copies land before the CTA exits
+        for (long long g = (issued > kGemmStages ? issued - kGemmStages : 0); g < issued; ++g)
+            wait_parity(s_u32(&full[g % kGemmStages]), (unsigned)((g / kGemmStages) & 1), nullptr);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+}
+
 // ---- surrogate training and inference kernels ------------------------------
 
 constexpr int kPatch = 64;             // height patch side (cells) around the voxel's pixel
@@ -580,6 +765,22 @@ cudaError_t launch_gemm_tiles(const void* A, const void* B, float* C, void* Cb, 
         e = cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmShape<BN>::kSmem);
         if (e != cudaSuccess) return e;
         attr[dev] = true;
+    }
+    const int tiles = (M / kTm) * (N / BN);
+    static int sms = 0;
+    if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+    if (!stall && tiles > sms && !getenv("SGB_GEMM_ONE_TILE_PER_CTA")) {
+        // more than one wave: persistent CTAs with two TMEM accumulators
+        static bool pattr[64] = {};
+        if (!pattr[dev]) {
+            e = cudaFuncSetAttribute(k_gemm_bf16_pers<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     GemmShape<BN>::kSmem);
+            if (e != cudaSuccess) return e;
+            pattr[dev] = true;
+        }
+        k_gemm_bf16_pers<BN><<<sms, kPersThreads, GemmShape<BN>::kSmem, st>>>(
+            mapA, mapB, C, static_cast<__nv_bfloat16*>(Cb), bias, M, N, K, relu, err);
+        return cudaGetLastError();
     }
     const dim3 grid(N / BN, M / kTm);
     k_gemm_bf16<BN><<<grid, kGemmThreads, GemmShape<BN>::kSmem, st>>>(

@@ -4,10 +4,12 @@ import pytest
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("bn", ["128", "256"])
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 320), (384, 256, 1024), (256, 512, 1600)])
+@pytest.mark.parametrize("bn", ["64", "128", "256"])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 320), (384, 256, 1024), (256, 512, 1600),
+                                   (5120, 1024, 320)])
 def test_gemm_bf16_matches_fp32_product(M, N, K, bn, monkeypatch):
-    """Both tile widths (SGB_GEMM_BN forces one where N allows it)."""
+    """Every tile width (SGB_GEMM_BN forces one where N allows it); the last
+    shape has more tiles than SMs, so it runs the persistent kernel."""
     monkeypatch.setenv("SGB_GEMM_BN", bn)
     import torch
     from solargpu_b200 import api
@@ -24,6 +26,24 @@ def test_gemm_bf16_matches_fp32_product(M, N, K, bn, monkeypatch):
     hb = torch.empty(M, N, dtype=torch.bfloat16, device="cuda")
     api.gemm_bf16(A, B, out_bf16=hb, bias=bias)
     torch.testing.assert_close(hb.float(), (want + bias).to(torch.bfloat16).float(), rtol=1e-2, atol=1e-2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bn", ["64", "256"])
+def test_persistent_gemm_equals_one_tile_per_cta(bn, monkeypatch):
+    """The persistent kernel (two TMEM accumulators, CTAs walking tiles)
+    issues the same MMAs in the same order as one CTA per tile: equal bits."""
+    import torch
+    from solargpu_b200 import api
+    monkeypatch.setenv("SGB_GEMM_BN", bn)
+    g = torch.Generator(device="cuda").manual_seed(9)
+    A = torch.randn(128 * 80, 448, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(512, 448, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(512, device="cuda", generator=g)
+    got = api.gemm_bf16(A, B, bias=bias, relu=True)
+    monkeypatch.setenv("SGB_GEMM_ONE_TILE_PER_CTA", "1")
+    want = api.gemm_bf16(A, B, bias=bias, relu=True)
+    assert torch.equal(got, want)
 
 
 def test_gemm_rejects_bad_shapes():
