@@ -22,6 +22,8 @@
 // bit-reproducible run to run.
 #include "solar_math.cuh"
 
+#include <atomic>
+
 namespace sgb {
 namespace {
 
@@ -376,12 +378,15 @@ k_reflect_group(int N, const float* __restrict__ slab, const long long* __restri
 
 int sm_count()
 {
-    static int sms = 0;
+    // shared by the threads of several contexts: written once, same value
+    static std::atomic<int> cached{0};
+    int sms = cached.load(std::memory_order_relaxed);
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 148;
+        cached.store(sms, std::memory_order_relaxed);
     }
     return sms;
 }

@@ -21,6 +21,8 @@
 // range; a malformed stream sets kErrBarleStream and stops that voxel.
 #include "solar_math.cuh"
 
+#include <atomic>
+
 namespace sgb {
 namespace {
 
@@ -368,12 +370,15 @@ __global__ void k_finalize_f64(const double* __restrict__ in, int N, float* __re
 
 int refl_grid(int N)
 {
-    static int sms = 0;
+    // shared by the threads of several contexts: written once, same value
+    static std::atomic<int> cached{0};
+    int sms = cached.load(std::memory_order_relaxed);
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 148;
+        cached.store(sms, std::memory_order_relaxed);
     }
     const long long need = ((long long)N + kReflWarps - 1) / kReflWarps;
     const long long cap = (long long)sms * 8;

@@ -22,6 +22,8 @@
 // M and N must be multiples of 128, K a multiple of 64 (the caller pads).
 #include "sgb_internal.cuh"
 
+#include <atomic>
+
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -756,27 +758,31 @@ cudaError_t launch_gemm_tiles(const void* A, const void* B, float* C, void* Cb, 
 {
     CUtensorMap mapA, mapB;
     if (!make_map(&mapA, A, M, K, kTm) || !make_map(&mapB, B, N, K, BN)) return cudaErrorInvalidValue;
-    static bool attr[64] = {};
+    static std::atomic<bool> attr[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!attr[dev]) {
+    if (!attr[dev].load(std::memory_order_acquire)) {
         e = cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmShape<BN>::kSmem);
         if (e != cudaSuccess) return e;
-        attr[dev] = true;
+        attr[dev].store(true, std::memory_order_release);
     }
     const int tiles = (M / kTm) * (N / BN);
-    static int sms = 0;
-    if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+    static std::atomic<int> sms_cached{0};
+    int sms = sms_cached.load(std::memory_order_relaxed);
+    if (!sms) {
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+        sms_cached.store(sms, std::memory_order_relaxed);
+    }
     if (!stall && tiles > sms && !getenv("SGB_GEMM_ONE_TILE_PER_CTA")) {
         // more than one wave: persistent CTAs with two TMEM accumulators
-        static bool pattr[64] = {};
-        if (!pattr[dev]) {
+        static std::atomic<bool> pattr[64];
+        if (!pattr[dev].load(std::memory_order_acquire)) {
             e = cudaFuncSetAttribute(k_gemm_bf16_pers<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      GemmShape<BN>::kSmem);
             if (e != cudaSuccess) return e;
-            pattr[dev] = true;
+            pattr[dev].store(true, std::memory_order_release);
         }
         k_gemm_bf16_pers<BN><<<sms, kPersThreads, GemmShape<BN>::kSmem, st>>>(
             mapA, mapB, C, static_cast<__nv_bfloat16*>(Cb), bias, M, N, K, relu, err);

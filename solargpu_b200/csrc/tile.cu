@@ -35,6 +35,8 @@
 // well) and returns.
 #include "solar_math.cuh"
 
+#include <atomic>
+
 namespace sgb {
 namespace {
 
@@ -615,28 +617,31 @@ k_reflect_tile(const float* __restrict__ slab, TileLists tl, const int* __restri
 
 int tile_sms()
 {
-    static int sms = 0;
+    // shared by the threads of several contexts: written once, same value
+    static std::atomic<int> cached{0};
+    int sms = cached.load(std::memory_order_relaxed);
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 148;
+        cached.store(sms, std::memory_order_relaxed);
     }
     return sms;
 }
 
 // Sets the dynamic shared-memory limit of a kernel once per device.
 template <typename K>
-cudaError_t allow_smem(K kernel, size_t bytes, bool (&done)[kMaxDevices])
+cudaError_t allow_smem(K kernel, size_t bytes, std::atomic<bool> (&done)[kMaxDevices])
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!done[dev]) {
+    if (!done[dev].load(std::memory_order_acquire)) {
         e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e != cudaSuccess) return e;
-        done[dev] = true;
+        done[dev].store(true, std::memory_order_release);
     }
     return cudaSuccess;
 }
@@ -647,7 +652,7 @@ cudaError_t tile_q(const float* slab, const TileLists& tl, const int* order, con
 {
     if (tl.R != StageLayout<Q>::R) return cudaErrorInvalidValue;
     const size_t smem = (size_t)kStages * StageLayout<Q>::kBytes;
-    static bool attr[kMaxDevices] = {};
+    static std::atomic<bool> attr[kMaxDevices];
     cudaError_t e = allow_smem(k_reflect_tile<Q>, smem, attr);
     if (e != cudaSuccess) return e;
     const int grid = tl.NG < tile_sms() ? tl.NG : tile_sms();
@@ -685,7 +690,7 @@ cudaError_t launch_tile_build(int NG, const int* start, const long long* woff, i
 {
     if (NG <= 0) return cudaSuccess;
     const size_t smem = (size_t)3 * kTileCap * 4;
-    static bool attr[kMaxDevices] = {};
+    static std::atomic<bool> attr[kMaxDevices];
     cudaError_t e = allow_smem(k_tile_build, smem, attr);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(rows_total, 0, sizeof(long long), st);
@@ -703,7 +708,7 @@ cudaError_t launch_tile_layout(int pass, int NG, int R, const int* start, const 
     if (NG <= 0) return cudaSuccess;
     if (R < 32) return cudaErrorInvalidValue;
     const size_t smem = layout_smem();
-    static bool attr0[kMaxDevices] = {}, attr1[kMaxDevices] = {};
+    static std::atomic<bool> attr0[kMaxDevices], attr1[kMaxDevices];
     cudaError_t e = pass == 0 ? allow_smem(k_tile_layout<0>, smem, attr0) : allow_smem(k_tile_layout<1>, smem, attr1);
     if (e != cudaSuccess) return e;
     if (pass == 0)
