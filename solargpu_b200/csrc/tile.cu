@@ -437,7 +437,7 @@ __device__ __forceinline__ void tile_accumulate(const Accum& a, int v, float x)
 template <int Q>
 struct StageLayout {
     static constexpr int kRowBytes = 32 * Q * 4;
-    static constexpr int kBudget = 108 * 1024;
+    static constexpr int kBudget = 113 * 1024;
     static constexpr int R = ((kBudget - kTabInts * 4) / (kRowBytes + kConsumerWarps * 18)) & ~7;
     static constexpr int kMaxEntries = kConsumerWarps * R;   // one entry per quad and row at most
     static constexpr int kW = R * kRowBytes;                  // float4 weights
