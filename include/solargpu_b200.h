@@ -192,6 +192,15 @@ int solar_gpu_run_lists(solar_gpu_context* ctx, const solar_gpu_options* opt, co
 int solar_gpu_trace_copy(solar_gpu_context* ctx, long long* csr_offsets, int* csr_ids,
                          long long* barle_offsets, unsigned char* barle_bytes, uint32_t* shadow);
 
+/* No counterpart in the reference.  Copies the part of the last Stage 1
+   result that belongs to voxels [v0, v1) (scenes whose full lists are too
+   large to copy): csr_offsets / barle_offsets [v1-v0+1] are the absolute
+   offsets offsets[v0..v1]; csr_ids and barle_bytes receive the entries
+   between offsets[v0] and offsets[v1] (size them from a first call that
+   passes NULL for them); shadow [v1-v0][shadow_words].  Any may be NULL. */
+int solar_gpu_trace_copy_range(solar_gpu_context* ctx, int v0, int v1, long long* csr_offsets, int* csr_ids,
+                               long long* barle_offsets, unsigned char* barle_bytes, uint32_t* shadow);
+
 /* Stage times of the last run, milliseconds, from CUDA events:
    [0] setup (tables, geometry), [1] Stage 1 (trace + lists),
    [2] Stage 2/3 (solar + reflection + accumulation), [3] total.
@@ -309,15 +318,18 @@ int solar_gpu_sg_transpose_f32(const float* in, int R, int C, float* out, void* 
    lists (device csr_offsets [num_lists+1] int64 from 0, device csr_ids
    int32) into device barle_offsets [num_lists+1] and device barle_bytes
    (capacity barle_capacity bytes); *barle_total (host) receives the byte
-   count, also when the capacity is too small (nothing is written then).
+   count, also when the capacity is too small (barle_offsets is filled then,
+   barle_bytes is left untouched).  Each list must hold distinct ids >= 1, as
+   the tracer's lists do; other lists are rejected (SOLAR_GPU_ERR_ARG).
    Bytes are identical to the library's own ba-RLE lists and to the reference
    encoder.  For callers that may not allocate device memory (their GPU memory
    is owned by a host framework's pool, or cudaMalloc/cudaFree stalls are not
    acceptable): it allocates nothing; its scratch is one fixed static device
    array of about 10.6 MB per device, so num_lists <= 1024 and each list
    <= 2592 ids.  Calls share that array: calls that overlap on the GPU race
-   and must be serialised.  The first call on a device looks up the array's
-   address; make it before any stream capture.  Runs on `stream` (NULL = the
+   and must be serialised.  The first call on a device (and the first after
+   the device's context was reset) looks up the array's address; make it
+   before any stream capture.  Runs on `stream` (NULL = the
    legacy default stream) and synchronises it. */
 int solar_gpu_barle_encode_noalloc(const long long* csr_offsets, const int* csr_ids, int num_lists,
                                    long long* barle_offsets, unsigned char* barle_bytes,

@@ -109,6 +109,49 @@ def trace(scene, bins: dict | None = None, v0: int = 0, v1: int | None = None,
     return off, out.astype(np.int32), sh
 
 
+def trace_list(scene, voxels: np.ndarray, bins: dict | None = None, lists: bool = True,
+               nthreads: int | None = None):
+    """DDA trace of an arbitrary voxel list (any order), each voxel exactly as
+    `trace` traces it.  Returns (off int64 [n+1], ids int32, shadow uint32
+    [n, words32]); with lists=False only the shadow words are kept (off and
+    ids are None), which needs no [n][D] buffer."""
+    if bins is None:
+        bins = sky_bins(scene.sun)
+    dirs, dense, upper = directions(bins)
+    vox = np.ascontiguousarray(voxels, np.int32)
+    n = vox.size
+    D = dirs.shape[0]
+    w32 = bins["words32"]
+    nthreads = nthreads or os.cpu_count() or 1
+    sh = np.zeros((n, w32), np.uint32)
+    wall = scene.wall_z if scene.wall_z.size else np.zeros(1, np.float32)
+    args = (_ptr(scene.grid), scene.width, scene.height, scene.num_total, scene.num_top,
+            _ptr(scene.pixel_parent), _ptr(wall), C.c_float(scene.max_height), _ptr(dirs), _ptr(dense),
+            _ptr(upper), D)
+    if not lists:
+        rc = lib().orc_trace_list(*args, _ptr(vox), n, None, None, sh.ctypes.data_as(_P), w32, 1, nthreads)
+        if rc != 0:
+            raise ValueError("voxel index out of range")
+        return None, None, sh
+    chunk = max(1, min(n, (1 << 28) // (D * 4)))
+    cnt_all = np.zeros(n, np.int32)
+    out = []
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        nb = np.zeros((b - a, D), np.int32)
+        cnt = np.zeros(b - a, np.int32)
+        rc = lib().orc_trace_list(*args, _ptr(vox[a:b]), b - a, _ptr(nb), _ptr(cnt), sh[a:b].ctypes.data_as(_P),
+                                  w32, 1, nthreads)
+        if rc != 0:
+            raise ValueError("voxel index out of range")
+        cnt_all[a:b] = cnt
+        out.append(nb[np.arange(D)[None, :] < cnt[:, None]])
+    off = np.zeros(n + 1, np.int64)
+    np.cumsum(cnt_all, out=off[1:])
+    ids = np.concatenate(out).astype(np.int32) if out else np.zeros(0, np.int32)
+    return off, ids, sh
+
+
 def trace_one(grid: np.ndarray, maxz: float, gx: int, gy: int, base_z: float, c, is_upper: bool,
               fma_mode: int = 1) -> int:
     """One DDA ray over a bare heightmap grid [H][W] from cell (gx, gy) at
@@ -194,6 +237,49 @@ def annual_fp64(scene, shadow: np.ndarray, off: np.ndarray, ids: np.ndarray, nth
                           _ptr(np.ascontiguousarray(ids, np.int32) if ids.size else np.zeros(1, np.int32)),
                           _ptr(out), _ptr(dd), nthreads or os.cpu_count() or 1)
     return out, dd
+
+
+def annual_fp64_sample(scene, sample, off, ids, shadow, cells, cell_shadow, nthreads=None) -> np.ndarray:
+    """FP64 annual irradiance (annual-sum form, as `annual_fp64`) of the
+    voxels `sample`, from their lists (off [n+1] from 0, ids 1-based cells)
+    and shadow words, given the shadow words of every top cell the lists name
+    (`cells`, ascending, 0-based)."""
+    sample = np.ascontiguousarray(sample, np.int32)
+    cells = np.ascontiguousarray(cells, np.int32)
+    sh = np.ascontiguousarray(shadow, np.uint32)
+    csh = np.ascontiguousarray(cell_shadow, np.uint32)
+    out = np.zeros(sample.size, np.float64)
+    wall = scene.wall_z if scene.wall_z.size else np.zeros(1, np.float32)
+    ids = np.ascontiguousarray(ids, np.int32)
+    nh = lib().orc_annual_fp64_sample(
+        _ptr(scene.grid), scene.width, scene.height, scene.num_total, scene.num_top,
+        _ptr(scene.pixel_parent), _ptr(wall), _ptr(scene.slopes), _ptr(scene.aspects),
+        _ptr(np.ascontiguousarray(scene.sun, np.float32)), _ptr(scene.direct), _ptr(scene.diffuse),
+        _ptr(sample), sample.size, _ptr(sh), _ptr(np.ascontiguousarray(off, np.int64)),
+        _ptr(ids if ids.size else np.zeros(1, np.int32)), _ptr(cells if cells.size else np.zeros(1, np.int32)),
+        cells.size, _ptr(csh if csh.size else np.zeros((1, sh.shape[1]), np.uint32)), sh.shape[1],
+        _ptr(out), nthreads or os.cpu_count() or 1)
+    if nh < 0:
+        raise ValueError("a list names a cell that is not in `cells`")
+    return out
+
+
+def sample_reference(scene, sample: np.ndarray, nthreads: int | None = None) -> dict:
+    """Everything the oracle needs to check a voxel sample of a scene too large
+    for a full CPU pass: the sample's own Stage 1 (lists + shadow words),
+    Stage 1 shadow words of every top cell its lists name, and the FP64 annual
+    irradiance of the sample from those oracle-built products."""
+    import time
+    bins = sky_bins(scene.sun)
+    t0 = time.perf_counter()
+    off, ids, sh = trace_list(scene, sample, bins, nthreads=nthreads)
+    cells = np.unique(ids.astype(np.int64) - 1).astype(np.int32)
+    _, _, csh = trace_list(scene, cells, bins, lists=False, nthreads=nthreads)
+    t1 = time.perf_counter()
+    tot = annual_fp64_sample(scene, sample, off, ids, sh, cells, csh, nthreads=nthreads)
+    t2 = time.perf_counter()
+    return dict(off=off, ids=ids, shadow=sh, cells=cells, cell_shadow=csh, annual=tot, bins=bins,
+                trace_s=t1 - t0, irradiance_s=t2 - t1)
 
 
 def hourly_fp64(scene, shadow, off, ids, v0=0, v1=None, hblock=64, nthreads=None):

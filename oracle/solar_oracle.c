@@ -868,7 +868,7 @@ static void* sample_trace_worker(void* arg)
     st.cur = 0;
     for (int i = j->a; i < j->b; ++i) {
         int v = j->sample[i];
-        int* out = j->nb + (size_t)i * s->D;
+        int* out = j->nb ? j->nb + (size_t)i * s->D : NULL;
         uint32_t* sh = j->sh + (size_t)i * j->words32;
         memset(sh, 0, sizeof(uint32_t) * (size_t)j->words32);
         ++st.cur;
@@ -877,9 +877,9 @@ static void* sample_trace_worker(void* arg)
             int hit = trace_ray(s, v, s->dirs[3 * d], s->dirs[3 * d + 1], s->dirs[3 * d + 2], s->upper[d]);
             if (!hit) continue;
             if (s->dense[d] >= 0) sh[s->dense[d] >> 5] |= 1u << (s->dense[d] & 31);
-            if (set_insert(&st, hit)) out[n++] = hit;
+            if (set_insert(&st, hit)) { if (out) out[n] = hit; ++n; }
         }
-        j->cnt[i] = n;
+        if (j->cnt) j->cnt[i] = n;
     }
     free(st.key); free(st.gen);
     return NULL;
@@ -1031,4 +1031,141 @@ int orc_trace_steps(const float* grid, int W, int H, int num_total, int num_top,
             steps[(size_t)i * D + d] = (short)(n > 32767 ? 32767 : n);
         }
     return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Sampled checks for scenes too large for a full CPU pass: Stage 1 of  */
+/* an arbitrary voxel list, and the FP64 annual irradiance of a voxel   */
+/* sample computed from oracle-built lists and shadow words.            */
+/* ------------------------------------------------------------------ */
+
+/* Traces the listed voxels (any order) exactly as orc_trace traces each
+   one: nb [n][D] first-occurrence lists (may be NULL), cnt [n] (may be
+   NULL), shadow [n][words32]. */
+int orc_trace_list(const float* grid, int W, int H, int num_total, int num_top,
+                   const int* pix_parent, const float* wall_z, float maxz,
+                   const float* dirs, const int* dense, const int* upper, int D,
+                   const int* voxels, int n, int* nb, int* cnt, uint32_t* shadow, int words32,
+                   int fma_mode, int nthreads)
+{
+    orc_scene s = { grid, W, H, num_total, num_top, pix_parent, wall_z, maxz,
+                    dirs, dense, upper, D, fma_mode };
+    if (n <= 0) return 0;
+    for (int i = 0; i < n; ++i)
+        if (voxels[i] < 0 || voxels[i] >= num_total) return -1;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > n) nthreads = n;
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+    sample_job* tj = (sample_job*)calloc((size_t)nthreads, sizeof(sample_job));
+    for (int t = 0; t < nthreads; ++t) {
+        tj[t].s = &s; tj[t].sample = voxels;
+        tj[t].a = (int)((long long)n * t / nthreads); tj[t].b = (int)((long long)n * (t + 1) / nthreads);
+        tj[t].nb = nb; tj[t].cnt = cnt; tj[t].sh = shadow; tj[t].words32 = words32;
+        pthread_create(&th[t], NULL, sample_trace_worker, &tj[t]);
+    }
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+    free(th); free(tj);
+    return 0;
+}
+
+typedef struct {
+    const orc_scene* s; const float *slopes, *aspects;
+    const orc_hour* hours; int nh; int words32;
+    const int* cells; int nc; const uint32_t* csh; double* at;   /* per listed top cell */
+    const int* sample; const uint32_t* sh; const long long* off; const int* ids;
+    int a, b; double* out; int missing;
+} subset_job;
+
+static void* subset_cell_worker(void* arg)
+{
+    subset_job* j = (subset_job*)arg;
+    for (int c = j->a; c < j->b; ++c) {
+        orc_vox g;
+        vox_geom(j->s, j->slopes, j->aspects, j->cells[c], &g);
+        double acc = 0.0;
+        for (int h = 0; h < j->nh; ++h)
+            acc += solar_I(&g, &j->hours[h], bit_of(j->csh, j->words32, c, j->hours[h].dense));
+        j->at[c] = acc;
+    }
+    return NULL;
+}
+
+static int find_cell(const int* cells, int nc, int x)
+{
+    int lo = 0, hi = nc - 1;
+    while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        if (cells[mid] == x) return mid;
+        if (cells[mid] < x) lo = mid + 1; else hi = mid - 1;
+    }
+    return -1;
+}
+
+static void* subset_voxel_worker(void* arg)
+{
+    subset_job* j = (subset_job*)arg;
+    for (int i = j->a; i < j->b; ++i) {
+        orc_vox me;
+        vox_geom(j->s, j->slopes, j->aspects, j->sample[i], &me);
+        double own = 0.0;
+        for (int h = 0; h < j->nh; ++h)
+            own += solar_I(&me, &j->hours[h], bit_of(j->sh, j->words32, i, j->hours[h].dense));
+        double r = 0.0;
+        for (long long k = j->off[i]; k < j->off[i + 1]; ++k) {
+            int ng = j->ids[k] - 1;
+            double w = refl_w(j->s, &me, ng);
+            if (w == 0.0) continue;
+            int c = find_cell(j->cells, j->nc, ng);
+            if (c < 0) { j->missing = 1; continue; }
+            r += w * j->at[c];
+        }
+        j->out[i] = own + r;
+    }
+    return NULL;
+}
+
+/* FP64 annual irradiance (Wh/m^2, the annual-sum form of orc_annual_fp64)
+   of the voxels sample[ns], from their first-occurrence lists (off [ns+1]
+   from 0, ids 1-based cells) and shadow words sh [ns][words32], given the
+   shadow words csh [nc][words32] of every top cell the lists name (cells
+   [nc], ascending).  out [ns].  Returns the daylight hour count, or -1 if a
+   list names a cell missing from `cells`. */
+int orc_annual_fp64_sample(const float* grid, int W, int H, int num_total, int num_top,
+                           const int* pix_parent, const float* wall_z,
+                           const float* slopes, const float* aspects,
+                           const float* sun_az_alt, const float* dni, const float* dhi,
+                           const int* sample, int ns, const uint32_t* sh, const long long* off, const int* ids,
+                           const int* cells, int nc, const uint32_t* csh, int words32,
+                           double* out, int nthreads)
+{
+    int fd[72 * 18 + 64], meta[5];
+    int* sdi = (int*)malloc(sizeof(int) * ORC_HOURS);
+    float* nudged = (float*)malloc(sizeof(float) * 2 * ORC_HOURS);
+    orc_hour* hours = (orc_hour*)malloc(sizeof(orc_hour) * ORC_HOURS);
+    orc_sky_bins(sun_az_alt, 5.0f, 5.0f, fd, sdi, nudged, meta);
+    int nh = orc_hour_table(nudged, sdi, dni, dhi, hours);
+    orc_scene s = { grid, W, H, num_total, num_top, pix_parent, wall_z, 0.0f, NULL, NULL, NULL, 0, 1 };
+    double* at = (double*)malloc(sizeof(double) * (size_t)(nc > 0 ? nc : 1));
+    if (nthreads < 1) nthreads = 1;
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+    subset_job* jobs = (subset_job*)calloc((size_t)nthreads, sizeof(subset_job));
+    int missing = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        int n = pass == 0 ? nc : ns;
+        for (int t = 0; t < nthreads; ++t) {
+            subset_job* j = &jobs[t];
+            j->s = &s; j->slopes = slopes; j->aspects = aspects; j->hours = hours; j->nh = nh;
+            j->words32 = words32; j->cells = cells; j->nc = nc; j->csh = csh; j->at = at;
+            j->sample = sample; j->sh = sh; j->off = off; j->ids = ids; j->out = out; j->missing = 0;
+            j->a = (int)((long long)n * t / nthreads);
+            j->b = (int)((long long)n * (t + 1) / nthreads);
+            pthread_create(&th[t], NULL, pass == 0 ? subset_cell_worker : subset_voxel_worker, j);
+        }
+        for (int t = 0; t < nthreads; ++t) {
+            pthread_join(th[t], NULL);
+            missing |= jobs[t].missing;
+        }
+    }
+    free(th); free(jobs); free(at); free(sdi); free(nudged); free(hours);
+    return missing ? -1 : nh;
 }

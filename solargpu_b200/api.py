@@ -95,6 +95,7 @@ def lib() -> C.CDLL:
         L.solar_gpu_trace.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), vp]
         L.solar_gpu_trace_sizes.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.solar_gpu_trace_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.solar_gpu_trace_copy_range.argtypes = [vp, i, i, vp, vp, vp, vp, vp]
         L.solar_gpu_run_lists.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), C.POINTER(ListsDesc), vp, vp]
         L.solar_gpu_gemm_bf16.argtypes = [vp, vp, vp, vp, vp, i, i, i, i, vp]
         L.solar_gpu_last_timings.argtypes = [vp, C.POINTER(C.c_double), i]
@@ -307,6 +308,27 @@ class Context:
         if b_off is not None:
             res["barle_off"], res["barle"] = b_off, b_bytes[:nb.value]
         res["shadow"] = shadow
+        return res
+
+    def trace_range(self, v0: int, v1: int, csr: bool = True, barle: bool = False) -> dict:
+        """The last Stage 1 result for voxels [v0, v1) only: offsets rebased
+        to 0, the lists and the shadow words (for scenes whose full lists are
+        too large to copy to the host)."""
+        L = lib()
+        n = v1 - v0
+        w = C.c_int()
+        _check(L.solar_gpu_trace_sizes(self.h, None, None, C.byref(w), None, None))
+        res = {"shadow": np.zeros((n, w.value), np.uint32)}
+        co = np.zeros(n + 1, np.int64) if csr else None
+        bo = np.zeros(n + 1, np.int64) if barle else None
+        _check(L.solar_gpu_trace_copy_range(self.h, v0, v1, _p(co), None, _p(bo), None, _p(res["shadow"])))
+        ids = np.zeros(max(1, int(co[-1] - co[0])), np.int32) if csr else None
+        byt = np.zeros(max(1, int(bo[-1] - bo[0])), np.uint8) if barle else None
+        _check(L.solar_gpu_trace_copy_range(self.h, v0, v1, None, _p(ids), None, _p(byt), None))
+        if csr:
+            res["csr_off"], res["csr_ids"] = co - co[0], ids[:int(co[-1] - co[0])]
+        if barle:
+            res["barle_off"], res["barle"] = bo - bo[0], byt[:int(bo[-1] - bo[0])]
         return res
 
     def timings(self) -> list[float]:

@@ -22,8 +22,16 @@
 //     without ordering between them) race on the array and corrupt each
 //     other's results -- serialise them;
 //   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and keeps it; make that
-//     first call before any stream capture on the device.
+//     cudaGetSymbolAddress (with that device current) and keeps it, keyed by
+//     the device's current CUDA context: after cudaDeviceReset, or once the
+//     primary context was destroyed and created again, the next call looks
+//     the address up again.  Make the first call in each context before any
+//     stream capture on the device;
+//   * each list must hold distinct ids >= 1 (the tracer's lists always do);
+//     the reference encoder would drop duplicates and stop at a 0, so such
+//     lists are rejected instead of being encoded differently.
+#include <cuda.h>
+
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -37,6 +45,7 @@ namespace {
 constexpr int kNoAllocLists = 1024;
 constexpr int kNoAllocRowLen = kMaxDirs;   // 2592: one id per traced direction at most
 constexpr int kMaxDevices = 64;
+constexpr int kErrBadIds = 1 << 16;         // a zero, negative or repeated id (this file's own flag bit)
 
 // Scratch layout (bytes): rows | counts | sizes | scan partial sums | error flag
 constexpr size_t kRowsBytes = sizeof(int) * (size_t)kNoAllocLists * kNoAllocRowLen;
@@ -63,12 +72,61 @@ __global__ void k_rows_from_csr(const long long* __restrict__ off, const int* __
         return;
     }
     int* row = rows + (size_t)i * kNoAllocRowLen;
-    for (long long k = lane; k < len; k += 32) row[k] = ids[s + k];
+    bool bad = false;
+    for (long long k = lane; k < len; k += 32) {
+        const int id = ids[s + k];
+        bad |= id < 1;
+        row[k] = id;
+    }
+    if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(err, kErrBadIds);
     if (lane == 0) counts[i] = (int)len;
 }
 
+// After the size pass each row holds its list sorted descending; a repeated
+// id shows up as two equal neighbours.
+__global__ void k_check_distinct(int n, const int* __restrict__ rows, const int* __restrict__ counts,
+                                 int* __restrict__ err)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int k = counts[i];
+    const int* row = rows + (size_t)i * kNoAllocRowLen;
+    bool dup = false;
+    for (int j = lane + 1; j < k; j += 32) dup |= row[j] == row[j - 1];
+    if (__any_sync(0xFFFFFFFFu, dup) && lane == 0) atomicOr(err, kErrBadIds);
+}
+
 std::mutex g_mu;
-unsigned char* g_addr[kMaxDevices] = {};   // device address of the scratch, per device ordinal
+unsigned char* g_addr[kMaxDevices] = {};              // device address of the scratch, per device ordinal
+unsigned long long g_ctx_id[kMaxDevices] = {};        // ...valid in the context with this id
+
+// Unique id of the calling thread's current context (cuCtxGetId: never reused
+// within a process), 0 if the driver cannot tell.
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {   // called under g_mu
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(p);
+        looked_up = true;
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
 
 int report(int code, const char* what, cudaError_t e)
 {
@@ -100,11 +158,15 @@ extern "C" int solar_gpu_barle_encode_noalloc(const long long* csr_offsets, cons
     unsigned char* base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_addr[dev]) {
+        // No context may be current yet on a first call: the lookup creates
+        // the primary context, and its id is read after it.
+        const unsigned long long ctx_id = current_context_id();
+        if (!g_addr[dev] || ctx_id == 0 || ctx_id != g_ctx_id[dev]) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);   // this device's copy of the array
             if (e != cudaSuccess) return report(SOLAR_GPU_ERR_CUDA, "cudaGetSymbolAddress", e);
             g_addr[dev] = static_cast<unsigned char*>(p);
+            g_ctx_id[dev] = current_context_id();
         }
         base = g_addr[dev];
     }
@@ -124,6 +186,9 @@ extern "C" int solar_gpu_barle_encode_noalloc(const long long* csr_offsets, cons
         if (e != cudaSuccess) return report(SOLAR_GPU_ERR_CUDA, "row copy", e);
         e = launch_barle_size(num_lists, kNoAllocRowLen, rows, counts, sizes, err, st);
         if (e != cudaSuccess) return report(SOLAR_GPU_ERR_CUDA, "size pass", e);
+        k_check_distinct<<<(num_lists * 32 + 255) / 256, 256, 0, st>>>(num_lists, rows, counts, err);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return report(SOLAR_GPU_ERR_CUDA, "id check", e);
     }
     e = launch_scan_counts(sizes, num_lists, 0, barle_offsets, scan, nullptr, st);
     if (e != cudaSuccess) return report(SOLAR_GPU_ERR_CUDA, "offset scan", e);
@@ -134,7 +199,11 @@ extern "C" int solar_gpu_barle_encode_noalloc(const long long* csr_offsets, cons
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return report(SOLAR_GPU_ERR_CUDA, "reading the stream size", e);
     *barle_total = total;
-    if (flag) return report(SOLAR_GPU_ERR_ARG, "a list is longer than 2592 ids", cudaSuccess);
+    if (flag & kErrListCapacity)
+        return report(SOLAR_GPU_ERR_ARG, "a list is longer than 2592 ids (or its offsets decrease)", cudaSuccess);
+    if (flag & kErrBadIds)
+        return report(SOLAR_GPU_ERR_ARG, "a list holds an id below 1 or the same id twice", cudaSuccess);
+    if (flag) return report(SOLAR_GPU_ERR_DEVICE_CHECK, "device check failed in the size pass", cudaSuccess);
     if (total > barle_capacity || (total > 0 && !barle_bytes))
         return report(SOLAR_GPU_ERR_ARG, "barle_capacity is smaller than *barle_total", cudaSuccess);
     if (num_lists > 0 && total > 0) {

@@ -1105,6 +1105,40 @@ int solar_gpu_trace_copy(solar_gpu_context* c, long long* csr_offsets, int* csr_
     return SOLAR_GPU_OK;
 }
 
+int solar_gpu_trace_copy_range(solar_gpu_context* c, int v0, int v1, long long* csr_offsets, int* csr_ids,
+                               long long* barle_offsets, unsigned char* barle_bytes, uint32_t* shadow)
+{
+    if (!c) return fail(SOLAR_GPU_ERR_ARG, "context is NULL");
+    if (v0 < 0 || v1 < v0 || v1 > c->N) return fail(SOLAR_GPU_ERR_ARG, "voxel range outside [0, num_voxels]");
+    CK(cudaSetDevice(c->device));
+    if ((csr_offsets || csr_ids) && !c->have_csr) return fail(SOLAR_GPU_ERR_ARG, "no CSR lists in the last trace");
+    if ((barle_offsets || barle_bytes) && !c->have_barle) return fail(SOLAR_GPU_ERR_ARG, "no ba-RLE lists in the last trace");
+    CK(cudaStreamSynchronize(c->own));
+    CK(cudaDeviceSynchronize());
+    const size_t n = (size_t)(v1 - v0);
+    long long a = 0, b = 0;
+    if (csr_offsets || csr_ids) {
+        CK(cudaMemcpy(&a, as<long long>(c->csr_off) + v0, sizeof(long long), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&b, as<long long>(c->csr_off) + v1, sizeof(long long), cudaMemcpyDeviceToHost));
+        if (csr_offsets)
+            CK(cudaMemcpy(csr_offsets, as<long long>(c->csr_off) + v0, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost));
+        if (csr_ids && b > a)
+            CK(cudaMemcpy(csr_ids, as<int>(c->csr_ids) + a, sizeof(int) * (size_t)(b - a), cudaMemcpyDeviceToHost));
+    }
+    if (barle_offsets || barle_bytes) {
+        CK(cudaMemcpy(&a, as<long long>(c->barle_off) + v0, sizeof(long long), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&b, as<long long>(c->barle_off) + v1, sizeof(long long), cudaMemcpyDeviceToHost));
+        if (barle_offsets)
+            CK(cudaMemcpy(barle_offsets, as<long long>(c->barle_off) + v0, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost));
+        if (barle_bytes && b > a)
+            CK(cudaMemcpy(barle_bytes, as<unsigned char>(c->barle_bytes) + a, (size_t)(b - a), cudaMemcpyDeviceToHost));
+    }
+    if (shadow && n)
+        CK(cudaMemcpy(shadow, as<uint32_t>(c->shadow) + (size_t)v0 * c->words32, sizeof(uint32_t) * n * c->words32,
+                      cudaMemcpyDeviceToHost));
+    return SOLAR_GPU_OK;
+}
+
 int solar_gpu_last_timings(solar_gpu_context* c, double* ms, int n)
 {
     if (!c || !ms) return fail(SOLAR_GPU_ERR_ARG, "NULL argument");

@@ -12,9 +12,15 @@ code, compiled from its sources by oracle/Makefile:
                           viewshed stage (include/cuda/viewshed_stage.cuh:37-125):
                           CSR ids, ba-RLE bytes, shadow bitmap
     ref_annual_<name>.npz the reference API's annual irradiance (both pipelines)
+    ref_stage1_blocks_dsm1024.npz
+                          per block of 4096 voxels of the 1024 x 1024 city, SHA-256
+                          digests of the reference viewshed stage's list lengths,
+                          CSR ids, ba-RLE sizes and bytes and shadow bitmap, plus a
+                          digest of the generated scene's arrays
 
     python tests/golden/make_golden.py host
     python tests/golden/make_golden.py gpu [--out DIR]
+    python tests/golden/make_golden.py gpu-large [--out DIR]
 """
 from __future__ import annotations
 
@@ -126,9 +132,48 @@ def gpu(out_dir: str):
     print("gpu fixtures written to", out_dir)
 
 
+BLOCK = 4096
+
+
+def scene_digest(s) -> str:
+    h = hashlib.sha256()
+    for a in (s.grid, s.pixel_parent, s.wall_z, s.slopes, s.aspects, s.sun, s.direct, s.diffuse):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def block_digests(off, ids, boff, barle, svf8, v0, v1) -> list[str]:
+    """Digests of voxels [v0, v1): list lengths (int32), CSR ids (int32),
+    ba-RLE sizes (int32), ba-RLE bytes, shadow bitmap in the reference layout
+    (uint8 [words8][v1 - v0])."""
+    return [sha(np.diff(off[v0:v1 + 1]).astype(np.int32)), sha(ids[off[v0]:off[v1]].astype(np.int32)),
+            sha(np.diff(boff[v0:v1 + 1]).astype(np.int32)), sha(barle[boff[v0]:boff[v1]].astype(np.uint8)),
+            sha(np.ascontiguousarray(svf8[:, v0:v1]))]
+
+
+def gpu_large(out_dir: str, name: str = "dsm1024"):
+    if O.ref_gpu() is None:
+        raise SystemExit("oracle/_ref/libsolarref.so is missing")
+    os.makedirs(out_dir, exist_ok=True)
+    s = inputs.make_scene(name)
+    r = O.ref_stage1(s)
+    n = s.num_total
+    dig = [block_digests(r["csr_off"], r["csr_ids"], r["barle_off"], r["barle"], r["svf"], v0, min(n, v0 + BLOCK))
+           for v0 in range(0, n, BLOCK)]
+    np.savez_compressed(os.path.join(out_dir, f"ref_stage1_blocks_{name}.npz"), block=BLOCK, num_total=n,
+                        scene=scene_digest(s), digests=np.array(dig), nnz=int(r["csr_ids"].size),
+                        barle_bytes=int(r["barle"].size), svf_words8=int(r["svf"].shape[0]))
+    print(name, "blocks", len(dig), "nnz", r["csr_ids"].size, "barle bytes", r["barle"].size)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["host", "gpu"])
+    ap.add_argument("what", choices=["host", "gpu", "gpu-large"])
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
-    host() if a.what == "host" else gpu(a.out)
+    if a.what == "host":
+        host()
+    elif a.what == "gpu":
+        gpu(a.out)
+    else:
+        gpu_large(a.out)

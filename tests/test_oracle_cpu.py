@@ -2,6 +2,7 @@
 reference's own code (golden fixtures made by tests/golden/make_golden.py)."""
 import hashlib
 import os
+import sys
 
 import numpy as np
 import pytest
@@ -124,6 +125,36 @@ def test_oracle_trace_matches_reference_gpu_golden(name):
     bytes_ = sh.view(np.uint8).reshape(s.num_total, -1)[:, :int(g["svf_words8"])]
     svf8[:] = bytes_.T
     assert hashlib.sha256(svf8.tobytes()).hexdigest() == str(g["sha_svf"])
+
+
+def test_oracle_trace_matches_reference_gpu_blocks_dsm1024():
+    """Oracle DDA on the 1024 x 1024 city against the reference CUDA viewshed
+    stage's own output (per-block digests made on a B200): three seeded blocks
+    of 4096 voxels (one of them the last, wall voxels), list lengths, CSR ids,
+    ba-RLE sizes and bytes and the shadow bitmap."""
+    path = os.path.join(GOLDEN, "ref_stage1_blocks_dsm1024.npz")
+    if not os.path.exists(path):
+        pytest.skip("reference GPU fixture not generated yet")
+    sys.path.insert(0, GOLDEN)
+    import make_golden as MG
+    from oracle import oracle as O
+    from solargpu_b200 import inputs
+    g = np.load(path)
+    s = inputs.make_scene("dsm1024")
+    assert MG.scene_digest(s) == str(g["scene"]), "the generator no longer makes the fixture's scene"
+    n, B = int(g["num_total"]), int(g["block"])
+    assert n == s.num_total
+    nb = (n + B - 1) // B
+    rng = np.random.default_rng(11)
+    bins = O.sky_bins(s.sun)
+    for b in sorted(set(rng.choice(nb - 1, 2, replace=False).tolist() + [nb - 1])):
+        v0, v1 = b * B, min(n, (b + 1) * B)
+        off, ids, sh = O.trace(s, bins, v0, v1)
+        boff, buf = O.barle_encode_csr(off, ids)
+        w8 = int(g["svf_words8"])
+        svf8 = np.ascontiguousarray(sh.view(np.uint8).reshape(v1 - v0, -1)[:, :w8].T)
+        got = MG.block_digests(off, ids, boff, buf, svf8, 0, v1 - v0)
+        assert got == [str(x) for x in g["digests"][b]], (b, v0, v1)
 
 
 def test_fp64_forms_agree(scene64):
