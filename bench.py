@@ -204,10 +204,18 @@ def roofline_bytes(scene, ctx_sizes, fmt, B, acc, V, entries, staged_rows=0) -> 
       V = 64 (tiles): merged entries of a 2-byte row index + the 4 weights of
              a voxel quad, the groups' union cell ids and chunk tables (80 B
              per chunk of 80 rows, ~1 B per staged row), offsets; slab rows of
-             every voxel."""
+             every voxel.
+      V = 128 (tensor cores): entries of 8 bytes (W-tile offset, fp16 hi and
+             lo) per nonzero weight, the union cell id of every staged row,
+             16 B of chunk offsets per 64 rows; per voxel the visiting-order
+             index, scale, normal, shadow words and accumulator; the fp16
+             slab of the top cells read once."""
     csr_entries, barle_bytes, words32 = ctx_sizes
     N, T = scene.num_total, scene.num_top
     acc_b = 16 if acc in (0, 1) else 8
+    if V == 128:
+        lists = entries * 8 + staged_rows * 4 + (staged_rows // 64) * 16 + 8 * (N + 1)
+        return float(lists + N * (4 + 4 + 16 + 4 * words32 + acc_b) + T * B * 2)
     if V == 0:
         lists = (barle_bytes if fmt == 1 else 4 * csr_entries) + 8 * (N + 1)
         return float(lists + N * (4 + 32 + 4 * words32 + acc_b) + T * B * 4)
@@ -494,7 +502,8 @@ def run_ours(args, world, rank, local, pg):
     # the line so that a stale figure can be told from a live one.
     traffic = None
     traffic_src = None
-    kname = "reflect_tile" if V >= 64 else "reflect_group" if V >= 1 else "reflect_block"
+    kname = ("reflect_mma" if V == 128 else "reflect_tile" if V >= 64 else "reflect_group" if V >= 1
+             else "reflect_block")
     prof = os.path.join("profiles", f"{kname}_{args.workload}_{FMT_NAMES[args.format].replace('-', '').lower()}_b{B}_v{V}.md")
     if os.path.exists(os.path.join(ROOT, prof)):
         for ln in open(os.path.join(ROOT, prof)):
@@ -504,7 +513,11 @@ def run_ours(args, world, rank, local, pg):
                     traffic_src = f"{prof} (ncu dram__bytes_read.sum + dram__bytes_write.sum, not measured in this run)"
                 except ValueError:
                     pass
-    if V >= 64:
+    if V == 128:
+        kdesc = ("k_reflect_mma (hour-block product on the tensor cores: tcgen05.mma kind::f16 M128 N256, "
+                 "128-voxel groups x 256 hours, union rows of the fp16 slab staged by cp.async into 128B-swizzled "
+                 "shared memory, split fp16 weights, FP32 accumulation in TMEM, + own term and accumulation)")
+    elif V >= 64:
         kdesc = (f"k_reflect_tile<{B // 32}> (hour-block sparse x dense product: union rows of {V}-voxel groups "
                  f"staged in shared memory by cp.async.bulk, merged 4-voxel entries, + accumulation)")
     elif V >= 1:
@@ -534,7 +547,21 @@ def run_ours(args, world, rank, local, pg):
                         "frac": round(flops / (per_launch_ms / 1e3) / 1e12 / fp32_peak, 4)
                         if fp32_peak and per_launch_ms > 0 else None,
                         "peak_note": "FP32 FMA pipe: SMs x 128 lanes x 2 flop x median SM clock under load"}
-    if V >= 64:
+    if V == 128:
+        # executed tensor-core work: two fp16 MMAs (weights hi and lo) of
+        # 128 voxels x 256 hours per staged union row
+        sm_mhz = clocks.get("sm_mhz") or 0.0
+        tens_peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1400.0)))
+        tens_src = ("measured" if "bf16_tflops_sustained" in peaks or "bf16_tflops" in peaks
+                    else "fallback (sustained under the power cap)")
+        dense = 2.0 * 128 * B * float(staged) * 2
+        roof["tensor"] = {"executed_flop_per_launch": dense,
+                          "achieved_tflops": round(dense / (per_launch_ms / 1e3) / 1e12, 1) if per_launch_ms > 0 else None,
+                          "peak_tflops": tens_peak, "peak_source": tens_src,
+                          "frac": round(dense / (per_launch_ms / 1e3) / 1e12 / tens_peak, 4) if per_launch_ms > 0 else None,
+                          "note": "dense fp16 MMA work including the zero weights of each group's union; the "
+                                  "useful work is the fp32 figure (one FMA per nonzero weight and hour)"}
+    if 64 <= V < 128:
         # the tile kernel's binding resource: shared-memory reads (one row of
         # B floats + the 18-byte entry per merged entry) against the SM data
         # path, 128 B per clock per SM at the median SM clock of the run
@@ -555,7 +582,7 @@ def run_ours(args, world, rank, local, pg):
     roof["hbm"] = {"achieved_gbs": roof["achieved"], "peak_gbs": hbm_peak, "frac": roof["frac"],
                    "peak_source": peak_src}
     cands = {"hbm": roof["frac"]}
-    for key in ("fp32", "smem"):
+    for key in ("fp32", "smem", "tensor"):
         if key in roof and roof[key].get("frac") is not None:
             cands[key] = roof[key]["frac"]
     bound = max(cands, key=cands.get)
@@ -563,6 +590,10 @@ def run_ours(args, world, rank, local, pg):
         roof.update({"bound": "fp32", "achieved": roof["fp32"]["achieved_tflops"],
                      "peak": roof["fp32"]["peak_tflops"], "unit": "TFLOP/s", "frac": roof["fp32"]["frac"],
                      "peak_source": "FP32 FMA pipe at the median SM clock (the kernel does not use tensor cores)"})
+    elif bound == "tensor":
+        roof.update({"bound": "tensor", "achieved": roof["tensor"]["achieved_tflops"],
+                     "peak": roof["tensor"]["peak_tflops"], "unit": "TFLOP/s", "frac": roof["tensor"]["frac"],
+                     "peak_source": roof["tensor"]["peak_source"]})
     elif bound == "smem":
         roof.update({"bound": "smem", "achieved": roof["smem"]["achieved_gbs"], "peak": roof["smem"]["peak_gbs"],
                      "unit": "GB/s", "frac": roof["smem"]["frac"],

@@ -90,7 +90,8 @@ struct solar_gpu_context {
         in_aspects, out_f32, order, order_cnt, order_cur, order_tmp, grp_cnt, grp_off, grp_tmp,
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
-        tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp;
+        tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -112,7 +113,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 65;
+static constexpr int kNumBufs = 74;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -243,7 +244,8 @@ int check_options(const solar_gpu_options* o, bool trace_only)
     case 8: ok = Bq >= 32 && Bq <= 128; break;
     case 1: case 2: ok = Bq >= 64 && Bq <= 512; break;
     case 64: ok = Bq >= 64 && Bq <= 256; break;
-    default: return fail(SOLAR_GPU_ERR_ARG, "group_size %d (0, 1, 2, 4, 8 or 64)", V);
+    case 128: ok = Bq == kMmaHours; break;
+    default: return fail(SOLAR_GPU_ERR_ARG, "group_size %d (0, 1, 2, 4, 8, 64 or 128)", V);
     }
     if (Bq > 1 && !ok)
         return fail(SOLAR_GPU_ERR_ARG, "hour_block %d is not built for group_size %d", Bq, V);
@@ -543,11 +545,16 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         const int slab_rows = o->group_size > 0 ? N : T;
         GroupLists gl{o->group_size, nullptr, nullptr, nullptr};
         TileLists tl{};
-        const bool tiled = o->group_size >= 64;
+        MmaLists ml{};
+        // group_size 128: the tensor-core kernel; a scene with a group whose
+        // union of neighbor cells exceeds the build's cap runs the shared-
+        // memory tile kernel (group_size 64) instead.
+        bool mma = o->group_size == kMmaGroup;
+        bool tiled = o->group_size >= 64;
         if (o->group_size > 0) {
             // Once per run: the nonzero weights of every list in visiting order,
             // then (V > 1) the merged union entries of each group of V voxels.
-            const int V = o->group_size;
+            int V = o->group_size;
             RK(ensure(c, c->w_cnt, sizeof(int) * (size_t)N));
             RK(ensure(c, c->w_off, sizeof(long long) * ((size_t)N + 1)));
             RK(ensure(c, c->w_tmp, sizeof(long long) * scan_scratch_elems(N)));
@@ -569,7 +576,76 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                                        as<int>(c->w_cell), as<float>(c->w_val), err, st));
             }
             c->launches += 5;
-            if (V == 1) {
+            if (mma) {
+                const int NG = mma_group_count(N);
+                RK(ensure(c, c->tile_slot, sizeof(unsigned short) * (size_t)(Ew + 1)));
+                RK(ensure(c, c->mma_union, sizeof(int) * (size_t)NG));
+                RK(ensure(c, c->mma_nch, sizeof(int) * (size_t)NG));
+                RK(ensure(c, c->mma_cbase, sizeof(long long) * ((size_t)NG + 1)));
+                RK(ensure(c, c->mma_over, sizeof(long long)));
+                {
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(cudaMemsetAsync(c->mma_over.p, 0, sizeof(long long), st));
+                    CK(launch_mma_union(N, as<long long>(c->w_off), as<int>(c->w_cell),
+                                        as<unsigned short>(c->tile_slot), as<int>(c->mma_union), as<int>(c->mma_nch),
+                                        as<int>(c->mma_over), st));
+                    CK(launch_scan_counts(as<int>(c->mma_nch), NG, 0, as<long long>(c->mma_cbase),
+                                          as<long long>(c->w_tmp), nullptr, st));
+                }
+                long long over = 0, C = 0;
+                RK(read_ll(c, as<long long>(c->mma_over), &over, st));
+                RK(read_ll(c, as<long long>(c->mma_cbase) + NG, &C, st));
+                c->launches += 4;
+                if (over != 0) {
+                    // the union build rewrote the cells of the groups it kept: rebuild the lists
+                    mma = false;
+                    V = 64;
+                    KScope k(c, SOLAR_GPU_KT_GROUP);
+                    CK(launch_weight_lists(1, g, N, T, nl, as<int>(c->order), nullptr, as<long long>(c->w_off),
+                                           as<int>(c->w_cell), as<float>(c->w_val), err, st));
+                    c->launches += 1;
+                } else {
+                    RK(ensure(c, c->mma_ccnt, sizeof(int) * (size_t)(C + 1)));
+                    RK(ensure(c, c->mma_coff, sizeof(long long) * ((size_t)C + 1)));
+                    RK(ensure(c, c->mma_scale, sizeof(float) * (size_t)N));
+                    RK(ensure(c, c->mma_ent, 8 * (size_t)(Ew + 1)));
+                    {
+                        KScope k(c, SOLAR_GPU_KT_GROUP);
+                        CK(launch_mma_layout(0, N, as<long long>(c->w_off), as<unsigned short>(c->tile_slot),
+                                             as<float>(c->w_val), as<int>(c->mma_nch), as<long long>(c->mma_cbase),
+                                             as<int>(c->mma_ccnt), nullptr, nullptr, as<float>(c->mma_scale), st));
+                        RK(ensure(c, c->chunk_tmp, sizeof(long long) * scan_scratch_elems((int)C)));
+                        CK(launch_scan_counts(as<int>(c->mma_ccnt), (int)C, 0, as<long long>(c->mma_coff),
+                                              as<long long>(c->chunk_tmp), nullptr, st));
+                        CK(launch_mma_layout(1, N, as<long long>(c->w_off), as<unsigned short>(c->tile_slot),
+                                             as<float>(c->w_val), as<int>(c->mma_nch), as<long long>(c->mma_cbase),
+                                             as<int>(c->mma_ccnt), as<long long>(c->mma_coff),
+                                             static_cast<uint2*>(c->mma_ent.p), as<float>(c->mma_scale), st));
+                    }
+                    c->launches += 3;
+                    c->group_entries = Ew;
+                    c->staged_rows = C * kMmaChunk;
+                    // weights and slots are dead now (see the tile path below)
+                    if (c->w_val.cap + c->tile_slot.cap > c->dev_total / 16) {
+                        CK(cudaFree(c->w_val.p));
+                        CK(cudaFree(c->tile_slot.p));
+                        c->w_val.p = c->tile_slot.p = nullptr;
+                        c->w_val.cap = c->tile_slot.cap = 0;
+                    }
+                    ml.N = N;
+                    ml.order = as<int>(c->order);
+                    ml.woff = as<long long>(c->w_off);
+                    ml.cells = as<int>(c->w_cell);
+                    ml.unions = as<int>(c->mma_union);
+                    ml.cbase = as<long long>(c->mma_cbase);
+                    ml.coff = as<long long>(c->mma_coff);
+                    ml.ent = c->mma_ent.p;
+                    ml.scale = as<float>(c->mma_scale);
+                }
+            }
+            if (mma) {
+                // built above
+            } else if (V == 1) {
                 c->group_entries = Ew;
                 gl.offsets = as<long long>(c->w_off);
                 gl.cells = as<int>(c->w_cell);
@@ -684,9 +760,15 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
             }
         }
         // allocated after the once-per-run builds, whose intermediates may
-        // have been released to make room (very large scenes)
-        RK(ensure(c, c->slab, sizeof(float) * (size_t)slab_rows * B));
-        float* slab = as<float>(c->slab);
+        // have been released to make room (very large scenes); the tensor-core
+        // kernel reads an fp16 slab of the top cells only
+        float* slab = nullptr;
+        if (mma) {
+            RK(ensure(c, c->slab16, 2 * (size_t)T * kMmaHours));
+        } else {
+            RK(ensure(c, c->slab, sizeof(float) * (size_t)slab_rows * B));
+            slab = as<float>(c->slab);
+        }
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         const bool use_graph = o->use_graph != 0 && !c->ktime;
@@ -695,11 +777,14 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
         for (int j0 = 0; j0 < Hd && le == cudaSuccess; j0 += B) {
             {
                 KScope k(c, SOLAR_GPU_KT_SOLAR);
-                le = launch_solar_slab(g, slab_rows, sh, c->words32, tab, j0, B, slab, st);
+                le = mma ? launch_solar_slab16(g, T, sh, c->words32, tab, j0, c->slab16.p, st)
+                         : launch_solar_slab(g, slab_rows, sh, c->words32, tab, j0, B, slab, st);
             }
             if (le == cudaSuccess) {
                 KScope k(c, SOLAR_GPU_KT_REFLECT);
-                if (tiled)
+                if (mma)
+                    le = launch_reflect_mma(c->slab16.p, ml, g, sh, c->words32, tab, j0, acc, err, st);
+                else if (tiled)
                     le = launch_reflect_tile(B, slab, tl, as<int>(c->order), acc, err, st);
                 else if (o->group_size > 0)
                     le = launch_reflect_group(N, B, slab, gl, as<int>(c->order), acc, st);
@@ -962,7 +1047,8 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_flag, &c->tile_pos, &c->tile_start, &c->tile_union, &c->tile_slot,
                                 &c->tile_rows, &c->tile_gcnt, &c->tile_gnch, &c->tile_gbase, &c->tile_tbase,
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
-                                &c->chunk_pos, &c->chunk_tmp};
+                                &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
+                                &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

@@ -203,4 +203,36 @@ cudaError_t launch_gemm_bf16(const void* A, const void* B, float* C, void* Cb, c
 cudaError_t launch_reflect_tile(int B, const float* slab, const TileLists& tl, const int* order, const Accum& acc,
                                 int* err, cudaStream_t st);
 
+// tensor-core reflection (mma.cu): groups of 128 visiting positions, hour
+// blocks of 256, fp16 slab of the top cells.
+struct MmaLists {
+    int N;
+    const int* order;          // [N] voxel at each visiting position
+    const long long* woff;     // [N + 1] weighted-list offsets; the union of group q starts at woff[128 q]
+    const int* cells;          // union cells per group (written over the weighted cells)
+    const int* unions;         // [groups] union size
+    const long long* cbase;    // [groups + 1] first chunk of each group
+    const long long* coff;     // [chunks + 1] first entry of each chunk
+    const void* ent;           // [entries] 8 bytes: W-tile byte offset, fp16 hi, fp16 lo
+    const float* scale;        // [N] per visiting position: 2^e undoing the weight scaling
+};
+constexpr int kMmaGroup = 128;
+constexpr int kMmaHours = 256;
+constexpr int kMmaChunk = 64;
+int mma_group_count(int N);
+// Union of each group (cells rewritten in place, slots per entry, union size
+// and chunk count per group); *over counts groups above the union cap.
+cudaError_t launch_mma_union(int N, const long long* woff, int* cells, unsigned short* slots, int* unions, int* nch,
+                             int* over, cudaStream_t st);
+// pass 0: entries per chunk (ccnt at cbase) and the per-position scale;
+// pass 1: the entries at coff (the scan of ccnt).
+cudaError_t launch_mma_layout(int pass, int N, const long long* woff, const unsigned short* slots, const float* wts,
+                              const int* nch, const long long* cbase, int* ccnt, const long long* coff, uint2* ent,
+                              float* scale, cudaStream_t st);
+cudaError_t launch_solar_slab16(const DevGeom& g, int T, const uint32_t* shadow, int words32, const HourEntry* table,
+                                int j0, void* slab16, cudaStream_t st);
+cudaError_t launch_reflect_mma(const void* slab16, const MmaLists& ml, const DevGeom& g, const uint32_t* shadow,
+                               int words32, const HourEntry* table, int j0, const Accum& acc, int* err,
+                               cudaStream_t st);
+
 }  // namespace sgb

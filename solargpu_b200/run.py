@@ -2,12 +2,13 @@
 
     python -m solargpu_b200.run --workload dsm1024 [--format 0] [--hour-block 256]
                                 [--group-size 64] [--accumulation 1] [--runs 2] [--out file.npy]
-                                [--compare-accumulation]
+                                [--dump file_voxels.bin] [--compare-accumulation]
 
 Plays the role of the reference CLI (src/main.cpp) for generated scenes:
 builds the seeded DSM, voxelizes it, computes the sun series and TMY, runs
 the CUDA pipeline `--runs` times on device-resident inputs and prints the
-stage and kernel-group times of the last run.  Also the profiling driver
+stage and kernel-group times of the last run; --out writes the top voxels'
+raster and --dump the reference's voxel dump (solargpu_b200/outputs.py).  Also the profiling driver
 (run it under ncu with -k/-s/-c filters).  --compare-accumulation runs the
 three accumulation modes (FP64 block sums, Kahan FP32, plain FP32) on the
 same scene and reports the relative differences of the last two from the
@@ -31,7 +32,8 @@ def main(argv=None) -> int:
     ap.add_argument("--accumulation", type=int, default=1)
     ap.add_argument("--chunk-voxels", type=int, default=0)
     ap.add_argument("--runs", type=int, default=2)
-    ap.add_argument("--out", default=None, help="write the annual irradiance (float32 .npy)")
+    ap.add_argument("--out", default=None, help="write the top voxels' annual irradiance raster (float32 .npy)")
+    ap.add_argument("--dump", default=None, help="write the voxel dump of the reference CLI (x, y, z, irradiance)")
     ap.add_argument("--compare-accumulation", action="store_true")
     a = ap.parse_args(argv)
 
@@ -75,8 +77,11 @@ def main(argv=None) -> int:
     print(json.dumps({"workload": a.workload, "voxels": s.num_total, "top_voxels": s.num_top,
                       "stage_ms": {"setup": round(t[0], 3), "stage1": round(t[1], 3), "stage23": round(t[2], 3),
                                    "total": round(t[3], 3)}, "kernel_group_ms": kt}))
+    from solargpu_b200 import outputs
     if a.out:
-        np.save(a.out, out.cpu().numpy())
+        outputs.write_raster(a.out, s, out.cpu().numpy())
+    if a.dump:
+        outputs.write_voxel_dump(a.dump, s, out.cpu().numpy())
     return 0
 
 

@@ -291,3 +291,29 @@ def test_dda_tie_steps_y_first():
     # stepping y first, the ray never enters (7, 6): it goes (6, 7), (7, 7), (7, 8), ...
     assert O.trace_one(_grid([(7, 6, 10.0)]), 10.0, 5, 5, 0.0, c, True) == 0
     assert O.trace_one(_grid([(7, 7, 10.0)]), 10.0, 5, 5, 0.0, c, True) == 7 + 7 * 16 + 1
+
+
+def test_voxel_dump_format(tmp_path, scene64):
+    """The voxel dump of the reference CLI (src/main.cpp:44-67): two int32
+    counts, then per voxel float32 x, y, z, irradiance; z is the cell height
+    for a top voxel and the wall height for a wall voxel."""
+    from solargpu_b200 import outputs
+    s = scene64
+    irr = np.linspace(1.0, 2.0, s.num_total).astype(np.float32)
+    p = str(tmp_path / "v.bin")
+    outputs.write_voxel_dump(p, s, irr)
+    raw = open(p, "rb").read()
+    assert len(raw) == 8 + 16 * s.num_total
+    n, t = np.frombuffer(raw[:8], "<i4")
+    assert (n, t) == (s.num_total, s.num_top)
+    rec = np.frombuffer(raw[8:], "<f4").reshape(-1, 4)
+    for i in (0, 1, s.num_top - 1, s.num_top, s.num_total - 1):
+        top = int(s.pixel_parent[i])
+        gx, gy = top % s.width, top // s.width
+        z = s.grid[gy * s.width + gx] if i < s.num_top else s.wall_z[i - s.num_top]
+        assert list(rec[i]) == [np.float32(gx), np.float32(gy), np.float32(z), irr[i]]
+    n2, t2, r2 = outputs.read_voxel_dump(p)
+    assert (n2, t2) == (n, t) and np.array_equal(r2["val"], irr)
+    outputs.write_raster(str(tmp_path / "r.npy"), s, irr)
+    r = np.load(str(tmp_path / "r.npy"))
+    assert r.shape == (s.height, s.width) and np.array_equal(r.ravel(), irr[:s.num_top])
