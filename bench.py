@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--format", type=int, default=0, help="0 = CSR, 1 = ba-RLE")
     ap.add_argument("--hour-block", type=int, default=256)
     ap.add_argument("--accumulation", type=int, default=1)
-    ap.add_argument("--group-size", type=int, default=64)
+    ap.add_argument("--group-size", type=int, default=128)
     ap.add_argument("--ref-workload", default=None,
                     help="reference arm: workload timed per step (default: the arm's own workload; its "
                          "uncompressed path takes 24 s per annual run of dsm1024, the compressed one ~6 min)")
@@ -348,7 +348,7 @@ def run_config3(args, ctx, dev, stream, flush) -> dict:
                     kt[g] = kt.get(g, 0.0) + t / runs
         return ms, kt
 
-    base = dict(hour_block=256, accumulation=api.ACC_KAHAN, group_size=64, use_graph=0, time_kernels=1)
+    base = dict(hour_block=256, accumulation=api.ACC_KAHAN, group_size=args.group_size, use_graph=0, time_kernels=1)
     res = {"workload": workload_desc(sc, args.config3_workload), "voxels": N, "daylight_hours": Hd,
            "host_generation_s": round(gen_s, 2),
            "reference": "unavailable at this size: the reference pipeline's int32 CSR / ba-RLE offsets "

@@ -62,12 +62,15 @@ typedef struct solar_gpu_options {
                                 their weighted lists merged once per run into union entries
                                 (B 64..512, 32..256, 32..128); 64 = groups of up to 64 voxels
                                 whose union rows are staged through shared memory, one CTA
-                                per group (B 64..256) */
+                                per group (B 64..256); 128 = groups of 128 voxels as a dense
+                                product on the tcgen05 tensor cores (fp16 slab, weights split
+                                into two fp16 parts, FP32 accumulation; B 256) */
 } solar_gpu_options;
 
 /* CSR lists, hour block 256, FP64 block sums, hourly reflection, chunk from
-   free memory, CUDA graph on, no kernel timing, group size 64 (the tile
-   kernel).  The drop-in entry points run with these, format aside. */
+   free memory, CUDA graph on, no kernel timing, group size 128 (the
+   tensor-core kernel).  The drop-in entry points run with these, format
+   aside. */
 void solar_gpu_default_options(solar_gpu_options* opt);
 
 /* ---- drop-in entry points (synchronous, host buffers, device 0) -------- */

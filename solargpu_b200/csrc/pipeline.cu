@@ -91,7 +91,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, bmax;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -105,6 +105,9 @@ struct solar_gpu_context {
     long long staged_rows = 0;   // slab rows the tile kernel stages per hour block
     long long weighted_entries = 0;   // nonzero reflection weights of the last run
     bool timed = false;
+    // a run released buffers to make room (scenes of tens of millions of
+    // voxels): the next run starts by releasing the Stage 2/3 buffers too
+    bool squeezed = false;
     // per kernel-group event log (time_kernels)
     bool ktime = false;
     std::vector<cudaEvent_t> kt_pool;
@@ -113,7 +116,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 74;
+static constexpr int kNumBufs = 75;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -378,7 +381,16 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         RK(ensure(c, c->barle_sizes, sizeof(int) * (size_t)N));
         RK(ensure(c, c->barle_bytes, (size_t)N * 160));
     }
-    const DevScene ds = dev_scene(s);
+    DevScene ds = dev_scene(s);
+    // max height of every 8 x 8 block: the tracer skips the height tests of
+    // blocks its ray passes above
+    RK(ensure(c, c->bmax, sizeof(float) * block_max_elems(s->grid_width, s->grid_height)));
+    {
+        KScope k(c, SOLAR_GPU_KT_SETUP);
+        CK(launch_block_max(s->grid, s->grid_width, s->grid_height, as<float>(c->bmax), st));
+    }
+    c->launches += 1;
+    ds.bmax = as<float>(c->bmax);
     // Rows follow the visiting order (Morton-adjacent voxels share a warp, so
     // their rays have similar lengths); with several chunks, each chunk (a
     // range of voxel indices) is traced in the visiting order of its voxels.
@@ -464,6 +476,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     // millions of voxels) is released here to leave room for Stage 2/3;
     // smaller ones are kept for the next call.
     if (c->raw.cap > c->dev_total / 4) {
+        c->squeezed = true;
         CK(cudaFree(c->raw.p));
         c->raw.p = nullptr;
         c->raw.cap = 0;
@@ -627,6 +640,7 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                     c->staged_rows = C * kMmaChunk;
                     // weights and slots are dead now (see the tile path below)
                     if (c->w_val.cap + c->tile_slot.cap > c->dev_total / 16) {
+                        c->squeezed = true;
                         CK(cudaFree(c->w_val.p));
                         CK(cudaFree(c->tile_slot.p));
                         c->w_val.p = c->tile_slot.p = nullptr;
@@ -713,6 +727,7 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 // device (scenes of tens of millions of voxels) they are
                 // released to make room for the slab.
                 if (c->w_val.cap + c->tile_slot.cap > c->dev_total / 16) {
+                    c->squeezed = true;
                     CK(cudaFree(c->w_val.p));
                     CK(cudaFree(c->tile_slot.p));
                     c->w_val.p = c->tile_slot.p = nullptr;
@@ -829,6 +844,21 @@ int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const sola
     RK(check_options(o, trace_only));
     if (!trace_only && !out) return fail(SOLAR_GPU_ERR_ARG, "irradiance output is NULL");
     CK(cudaSetDevice(c->device));
+    if (c->squeezed) {
+        // The previous run released buffers to fit: the Stage 2/3 buffers it
+        // still holds (slabs, weighted lists, group layouts) are rebuilt by
+        // every run, and holding them would leave no room for Stage 1.
+        CK(cudaStreamSynchronize(st));
+        DevBuf* stage23[] = {&c->slab, &c->slab16, &c->w_cnt, &c->w_off, &c->w_cell, &c->w_val, &c->grp_cell,
+                             &c->grp_w, &c->tile_slot, &c->tile_erow, &c->tile_ew, &c->tile_table, &c->mma_ent,
+                             &c->mma_ccnt, &c->mma_coff, &c->mma_scale, &c->hourly};
+        for (DevBuf* b : stage23) {
+            if (b->p) CK(cudaFree(b->p));
+            b->p = nullptr;
+            b->cap = 0;
+        }
+        c->squeezed = false;
+    }
     c->launches = 0;
     c->timed = false;
     c->ktime = o->time_kernels != 0;
@@ -1007,7 +1037,7 @@ void solar_gpu_default_options(solar_gpu_options* o)
     o->chunk_voxels = 0;
     o->use_graph = 1;
     o->time_kernels = 0;
-    o->group_size = 64;
+    o->group_size = kMmaGroup;
 }
 
 const char* solar_gpu_last_error(void) { return g_err.c_str(); }
@@ -1048,7 +1078,8 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_rows, &c->tile_gcnt, &c->tile_gnch, &c->tile_gbase, &c->tile_tbase,
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
-                                &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16};
+                                &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
+                                &c->bmax};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

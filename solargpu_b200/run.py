@@ -1,7 +1,7 @@
 """Command-line runner: the annual irradiance path on a named synthetic workload.
 
     python -m solargpu_b200.run --workload dsm1024 [--format 0] [--hour-block 256]
-                                [--group-size 64] [--accumulation 1] [--runs 2] [--out file.npy]
+                                [--group-size 128] [--accumulation 1] [--runs 2] [--out file.npy]
                                 [--dump file_voxels.bin] [--compare-accumulation]
 
 Plays the role of the reference CLI (src/main.cpp) for generated scenes:
@@ -28,7 +28,7 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", default="dsm1024")
     ap.add_argument("--format", type=int, default=0, help="0 = CSR, 1 = ba-RLE")
     ap.add_argument("--hour-block", type=int, default=256)
-    ap.add_argument("--group-size", type=int, default=64)
+    ap.add_argument("--group-size", type=int, default=128)
     ap.add_argument("--accumulation", type=int, default=1)
     ap.add_argument("--chunk-voxels", type=int, default=0)
     ap.add_argument("--runs", type=int, default=2)

@@ -31,9 +31,10 @@ import numpy as np
 
 from . import inputs
 
-CANDIDATES = tuple(dict(neighbor_format=f, hour_block=b, group_size=g)
-                   for f in (0, 1) for b in (128, 256) for g in (1, 64))
-DEFAULT = dict(neighbor_format=0, hour_block=256, group_size=64)
+CANDIDATES = (tuple(dict(neighbor_format=f, hour_block=b, group_size=g)
+                    for f in (0, 1) for b in (128, 256) for g in (1, 64))
+              + tuple(dict(neighbor_format=f, hour_block=256, group_size=128) for f in (0, 1)))
+DEFAULT = dict(neighbor_format=0, hour_block=256, group_size=128)
 
 
 def tile_configs(n: int = 32, seed: int = 0) -> list[inputs.DsmConfig]:
