@@ -201,6 +201,10 @@ int solar_gpu_trace_copy(solar_gpu_context* ctx, long long* csr_offsets, int* cs
    offsets offsets[v0..v1]; csr_ids and barle_bytes receive the entries
    between offsets[v0] and offsets[v1] (size them from a first call that
    passes NULL for them); shadow [v1-v0][shadow_words].  Any may be NULL. */
+/* After a full run (solar_gpu_run_device / solar_gpu_run_host) of a scene so
+   large that Stage 1's raw hit rows exceed a quarter of the device memory,
+   the lists are released once the weighted lists are built, to make room for
+   the hour loop; solar_gpu_trace (Stage 1 alone) always keeps them. */
 int solar_gpu_trace_copy_range(solar_gpu_context* ctx, int v0, int v1, long long* csr_offsets, int* csr_ids,
                                long long* barle_offsets, unsigned char* barle_bytes, uint32_t* shadow);
 

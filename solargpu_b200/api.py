@@ -284,6 +284,13 @@ class Context:
                        int(lists["shadow_words"]), int(lists["active_bins"]))
         _check(lib().solar_gpu_run_lists(self.h, C.byref(o), C.byref(d), C.byref(ld), _p(out), stream))
 
+    def stage1(self, scene, dev: dict, neighbor_format: int = BOTH, stream=None, **opts) -> None:
+        """Runs Stage 1 only and keeps its products on the device (read them
+        with `trace_range`)."""
+        o = options(neighbor_format=neighbor_format, **opts)
+        d, keep = _scene_desc(scene, dev)
+        _check(lib().solar_gpu_trace(self.h, C.byref(o), C.byref(d), stream))
+
     def trace(self, scene, dev: dict, neighbor_format: int = BOTH, stream=None, **opts) -> dict:
         """Runs Stage 1 and returns its lists and shadow words as numpy arrays."""
         o = options(neighbor_format=neighbor_format, **opts)

@@ -364,6 +364,43 @@ struct MmaTiles {
     const float* scale;        // [N] 2^e per visiting position
 };
 
+// Walks the (group, chunk) sequence of one CTA: groups blockIdx.x,
+// blockIdx.x + gridDim.x, ..., chunks of 64 union rows inside each group
+// (groups with an empty union have none) -- the order every role follows.
+struct Cursor {
+    int q, c, u, step, NG;
+    long long ub;   // first union cell of group q
+    __device__ Cursor(const MmaTiles& mt, int first, int stride) : q(first), c(0), u(0), step(stride), NG(mt.NG), ub(0)
+    {
+        settle(mt);
+    }
+    __device__ bool valid() const { return q < NG; }
+    __device__ void settle(const MmaTiles& mt)
+    {
+        for (; q < NG; q += step, c = 0) {
+            u = __ldg(mt.unions + q);
+            if (c * kChunk < u) break;
+        }
+        if (q < NG) ub = __ldg(mt.woff + (long long)q * kGroup);
+    }
+    __device__ void advance(const MmaTiles& mt)
+    {
+        ++c;
+        if (c * kChunk >= u) {
+            q += step;
+            c = 0;
+            settle(mt);
+        }
+    }
+    // cell of row r of the current chunk (padding rows repeat row 0: their weights are 0)
+    __device__ int row_cell(const MmaTiles& mt, int r, bool want) const
+    {
+        if (!want) return 0;
+        const int rows = min(kChunk, u - c * kChunk);
+        return __ldg(mt.cells + ub + (long long)c * kChunk + (r < rows ? r : 0));
+    }
+};
+
 __global__ void __launch_bounds__(kThreads, 1)
 k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __restrict__ geo_n,
               const uint32_t* __restrict__ shadow, int words32, const HourEntry* __restrict__ table, int j0,
@@ -407,42 +444,42 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
     bool ok = true;
 
     if (warp < kProducerWarps) {
-        // ---- producers: 16 rows a warp, one 16-byte piece a lane per row
+        // ---- producers: 16 rows a warp, one 16-byte piece a lane per row; the
+        // cell ids of the next chunk are loaded while this one is issued
         long long k = 0;
         const int r0 = warp * 16;
-        for (int q = blockIdx.x; q < mt.NG && ok; q += gridDim.x) {
-            const int u = mt.unions[q];
-            const long long ub = mt.woff[(long long)q * kGroup];
-            for (int c = 0; c * kChunk < u && ok; ++c, ++k) {
-                const int s = (int)(k % kStages);
-                const bool w_ok = k < kStages || bar_wait(su32(&empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_fail);
-                if (!__all_sync(0xFFFFFFFFu, w_ok)) {   // the warp decides as one
-                    ok = false;
-                    break;
-                }
-                const int rows = min(kChunk, u - c * kChunk);
-                // padding rows repeat the chunk's first row (their weights are 0)
-                const int my = lane < 16 ? __ldg(mt.cells + ub + c * kChunk + (r0 + lane < rows ? r0 + lane : 0)) : 0;
-                const unsigned bst = base + (unsigned)(s * kStageBytes) + 2 * kTileA;
-                const int na = lane >> 3, cc = lane & 7;
-#pragma unroll 4
-                for (int i = 0; i < 16; ++i) {
-                    const int kr = r0 + i;
-                    const int cell = __shfl_sync(0xFFFFFFFFu, my, i);
-                    const __half* src = slab + (size_t)cell * kHours + lane * 8;
-                    const int r8 = kr & 7;
-                    const unsigned dst = bst + (unsigned)(na * 8192 + (kr >> 3) * 1024 + r8 * 128 + ((cc ^ r8) << 4));
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-                }
-                asm volatile("cp.async.commit_group;" ::: "memory");
-                if (k >= 1) {
-                    // the previous chunk's copies have landed: publish them to the tensor cores
-                    asm volatile("cp.async.wait_group 1;" ::: "memory");
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) bar_arrive(su32(&full[(k - 1) % kStages]));
-                }
+        Cursor cur(mt, blockIdx.x, gridDim.x);
+        int my = cur.valid() ? cur.row_cell(mt, r0 + lane, lane < 16) : 0;
+        while (cur.valid() && ok) {
+            const int s = (int)(k % kStages);
+            const bool w_ok = k < kStages || bar_wait(su32(&empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_fail);
+            if (!__all_sync(0xFFFFFFFFu, w_ok)) {   // the warp decides as one
+                ok = false;
+                break;
             }
+            const int cur_cell = my;
+            cur.advance(mt);
+            my = cur.valid() ? cur.row_cell(mt, r0 + lane, lane < 16) : 0;
+            const unsigned bst = base + (unsigned)(s * kStageBytes) + 2 * kTileA;
+            const int na = lane >> 3, cc = lane & 7;
+#pragma unroll 4
+            for (int i = 0; i < 16; ++i) {
+                const int kr = r0 + i;
+                const int cell = __shfl_sync(0xFFFFFFFFu, cur_cell, i);
+                const __half* src = slab + (size_t)cell * kHours + lane * 8;
+                const int r8 = kr & 7;
+                const unsigned dst = bst + (unsigned)(na * 8192 + (kr >> 3) * 1024 + r8 * 128 + ((cc ^ r8) << 4));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            if (k >= 1) {
+                // the previous chunk's copies have landed: publish them to the tensor cores
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) bar_arrive(su32(&full[(k - 1) % kStages]));
+            }
+            ++k;
         }
         asm volatile("cp.async.wait_group 0;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -494,36 +531,61 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         }
         __syncwarp();
     } else if (warp >= kBuilderWarp0) {
-        // ---- builders: zero the W tiles, scatter the chunk's weights
+        // ---- builders: zero the W tiles, scatter the chunk's weights; the
+        // entries of the next chunk are loaded into registers while the
+        // builders wait for its stage
         const int bt = threadIdx.x - kBuilderWarp0 * 32;
         constexpr int kBuilders = kBuilderWarps * 32;
-        long long k = 0;
-        for (int q = blockIdx.x; q < mt.NG && ok; q += gridDim.x) {
-            const int u = mt.unions[q];
-            const long long cb = mt.cbase[q];
-            for (int c = 0; c * kChunk < u; ++c, ++k) {
-                const int s = (int)(k % kStages);
-                // one thread waits for the stage; every builder takes its decision
-                if (bt == 0)
-                    s_bok = (k < kStages || bar_wait(su32(&empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_fail))
-                                ? 1 : 0;
-                asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
-                ok = s_bok != 0;
-                if (!ok) break;
-                unsigned char* sa = gbase + (size_t)s * kStageBytes;
-                uint4* z = reinterpret_cast<uint4*>(sa);
-                for (int i = bt; i < 2 * kTileA / 16; i += kBuilders) z[i] = make_uint4(0u, 0u, 0u, 0u);
-                asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
-                const long long e0 = mt.coff[cb + c], e1 = mt.coff[cb + c + 1];
-                for (long long e = e0 + bt; e < e1; e += kBuilders) {
-                    const uint2 en = __ldg(mt.ent + e);
-                    *reinterpret_cast<unsigned short*>(sa + en.x) = (unsigned short)(en.y & 0xFFFFu);
-                    *reinterpret_cast<unsigned short*>(sa + kTileA + en.x) = (unsigned short)(en.y >> 16);
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
-                if (bt == 0) bar_arrive(su32(&aready[s]));
+        constexpr int kPref = 12;   // entries a thread holds ahead; more are loaded at scatter time
+        Cursor cur(mt, blockIdx.x, gridDim.x);
+        uint2 pre[kPref];
+        long long pe0 = 0, pe1 = 0;
+        auto prefetch = [&]() {
+            pe0 = pe1 = 0;
+            if (cur.valid()) {
+                const long long ci = __ldg(mt.cbase + cur.q) + cur.c;
+                pe0 = __ldg(mt.coff + ci);
+                pe1 = __ldg(mt.coff + ci + 1);
             }
+#pragma unroll
+            for (int i = 0; i < kPref; ++i) {
+                const long long e = pe0 + bt + (long long)i * kBuilders;
+                pre[i] = e < pe1 ? __ldg(mt.ent + e) : make_uint2(0xFFFFFFFFu, 0u);
+            }
+        };
+        prefetch();
+        long long k = 0;
+        while (cur.valid() && ok) {
+            const int s = (int)(k % kStages);
+            // one thread waits for the stage; every builder takes its decision
+            if (bt == 0)
+                s_bok = (k < kStages || bar_wait(su32(&empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_fail))
+                            ? 1 : 0;
+            asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
+            ok = s_bok != 0;
+            if (!ok) break;
+            unsigned char* sa = gbase + (size_t)s * kStageBytes;
+            uint4* z = reinterpret_cast<uint4*>(sa);
+            for (int i = bt; i < 2 * kTileA / 16; i += kBuilders) z[i] = make_uint4(0u, 0u, 0u, 0u);
+            asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
+#pragma unroll
+            for (int i = 0; i < kPref; ++i) {
+                if (pre[i].x != 0xFFFFFFFFu) {
+                    *reinterpret_cast<unsigned short*>(sa + pre[i].x) = (unsigned short)(pre[i].y & 0xFFFFu);
+                    *reinterpret_cast<unsigned short*>(sa + kTileA + pre[i].x) = (unsigned short)(pre[i].y >> 16);
+                }
+            }
+            for (long long e = pe0 + bt + (long long)kPref * kBuilders; e < pe1; e += kBuilders) {
+                const uint2 en = __ldg(mt.ent + e);
+                *reinterpret_cast<unsigned short*>(sa + en.x) = (unsigned short)(en.y & 0xFFFFu);
+                *reinterpret_cast<unsigned short*>(sa + kTileA + en.x) = (unsigned short)(en.y >> 16);
+            }
+            cur.advance(mt);
+            prefetch();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
+            if (bt == 0) bar_arrive(su32(&aready[s]));
+            ++k;
         }
         if (!ok) {
             if (bt == 0) atomicOr(err, kErrWaitTimeout);

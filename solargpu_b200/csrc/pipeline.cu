@@ -91,7 +91,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, bmax;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -116,7 +116,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 75;
+static constexpr int kNumBufs = 74;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -381,16 +381,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         RK(ensure(c, c->barle_sizes, sizeof(int) * (size_t)N));
         RK(ensure(c, c->barle_bytes, (size_t)N * 160));
     }
-    DevScene ds = dev_scene(s);
-    // max height of every 8 x 8 block: the tracer skips the height tests of
-    // blocks its ray passes above
-    RK(ensure(c, c->bmax, sizeof(float) * block_max_elems(s->grid_width, s->grid_height)));
-    {
-        KScope k(c, SOLAR_GPU_KT_SETUP);
-        CK(launch_block_max(s->grid, s->grid_width, s->grid_height, as<float>(c->bmax), st));
-    }
-    c->launches += 1;
-    ds.bmax = as<float>(c->bmax);
+    const DevScene ds = dev_scene(s);
     // Rows follow the visiting order (Morton-adjacent voxels share a warp, so
     // their rays have similar lengths); with several chunks, each chunk (a
     // range of voxel indices) is traced in the visiting order of its voxels.
@@ -774,6 +765,19 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 gl.weights = as<float>(c->grp_w);
             }
         }
+        if (o->group_size > 0 && c->squeezed) {
+            // Very large scenes: the hour loop reads only the weighted lists
+            // (or the group layouts built from them), so the CSR / ba-RLE
+            // lists are released to make room for the slab; solar_gpu_trace
+            // (Stage 1 alone) keeps them.
+            CK(cudaStreamSynchronize(st));
+            for (DevBuf* b : {&c->csr_ids, &c->barle_bytes}) {
+                if (b->p) CK(cudaFree(b->p));
+                b->p = nullptr;
+                b->cap = 0;
+            }
+            c->have_csr = c->have_barle = false;
+        }
         // allocated after the once-per-run builds, whose intermediates may
         // have been released to make room (very large scenes); the tensor-core
         // kernel reads an fp16 slab of the top cells only
@@ -851,13 +855,14 @@ int run_device_impl(solar_gpu_context* c, const solar_gpu_options* o, const sola
         CK(cudaStreamSynchronize(st));
         DevBuf* stage23[] = {&c->slab, &c->slab16, &c->w_cnt, &c->w_off, &c->w_cell, &c->w_val, &c->grp_cell,
                              &c->grp_w, &c->tile_slot, &c->tile_erow, &c->tile_ew, &c->tile_table, &c->mma_ent,
-                             &c->mma_ccnt, &c->mma_coff, &c->mma_scale, &c->hourly};
+                             &c->mma_ccnt, &c->mma_coff, &c->mma_scale, &c->hourly, &c->csr_ids, &c->barle_bytes};
         for (DevBuf* b : stage23) {
             if (b->p) CK(cudaFree(b->p));
             b->p = nullptr;
             b->cap = 0;
         }
         c->squeezed = false;
+        c->have_csr = c->have_barle = false;
     }
     c->launches = 0;
     c->timed = false;
@@ -1078,8 +1083,7 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_rows, &c->tile_gcnt, &c->tile_gnch, &c->tile_gbase, &c->tile_tbase,
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
-                                &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
-                                &c->bmax};
+                                &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

@@ -50,7 +50,6 @@ struct DevScene {
     const float* aspects;     // [N]
     int W, H, N, T;
     float maxz;
-    const float* bmax = nullptr;   // [ceil(H/8)][ceil(W/8)] max height of each 8 x 8 block, or nullptr
 };
 
 // Per-voxel geometry derived once per call.
@@ -76,10 +75,6 @@ cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int wor
                          const int* perm, cudaStream_t st);
 cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, const int* perm,
                           cudaStream_t st);
-// bmax[(y / 8) * ceil(W / 8) + x / 8] = max height of the 8 x 8 block (the
-// tracer skips the height test of a cell whose block cannot be hit).
-size_t block_max_elems(int W, int H);
-cudaError_t launch_block_max(const float* grid, int W, int H, float* bmax, cudaStream_t st);
 cudaError_t launch_invert(const int* perm, int n, int* inv, cudaStream_t st);
 // perm = the chunk voxels [v0, v0 + n) (as v - v0) in visiting order;
 // flag [N] and pos [N + 1] scratch.

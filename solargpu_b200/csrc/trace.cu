@@ -29,17 +29,9 @@ constexpr int kDedupeWarps = 4;
 constexpr int kHashSlots = 4096;   // > 2592 possible distinct hits per voxel
 constexpr int kDedupeBatch = 9;    // 2592 = 9 batches of 9 rounds of 32 directions
 
-constexpr int kBlockShift = 3;   // 8 x 8 cells per block of the block-max grid
-
-// With SKIP, the height test of a cell is made only when the max height of
-// its 8 x 8 block could hit: grid[c] <= bmax and fsub is monotonic, so
-// fsub(bmax, zr) <= 0.01 implies fsub(grid[c], zr) <= 0.01 for every cell of
-// the block -- the skipped tests are exactly the ones that would fail, and
-// the hit cell is unchanged.  The block index follows the DDA with per-axis
-// counters; a block's max is loaded once per block entered.
-template <bool UP, bool SKIP>
-__device__ __forceinline__ int trace_ray(const float* __restrict__ grid, const float* __restrict__ bmax, int W, int H,
-                                         float maxz, int gx, int gy, float base_z, const DirEntry& d)
+template <bool UP>
+__device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, int H, float maxz, int gx, int gy,
+                                         float base_z, const DirEntry& d)
 {
     // Cdir * 2.0f is exact, so these match the reference fused or not.
     const float ox = __fadd_rn((float)gx, __fmul_rn(d.cx, 2.0f));
@@ -66,58 +58,20 @@ __device__ __forceinline__ int trace_ray(const float* __restrict__ grid, const f
     int left_y = py ? H - 1 - iy : iy;
     const int step_y = py ? W : -W;
     int cell = ix + iy * W;
-    if constexpr (!SKIP) {
-        for (;;) {
-            const float zr = __fmaf_rn(d.cz, t, oz);
-            if (UP ? (zr > maxz) : (zr < 0.0f)) return 0;
-            if (__fsub_rn(__ldg(grid + cell), zr) > 0.01f) return cell + 1;
-            if (tMaxX < tMaxY) {
-                if (--left_x < 0) return 0;
-                t = tMaxX; cell += sx; tMaxX = __fadd_rn(tMaxX, d.dX);
-            } else {
-                if (--left_y < 0) return 0;
-                t = tMaxY; cell += step_y; tMaxY = __fadd_rn(tMaxY, d.dY);
-            }
-        }
-    } else {
-        constexpr int kB = 1 << kBlockShift;
-        const int bw = (W + kB - 1) >> kBlockShift;
-        int bx_left = px ? (kB - 1) - (ix & (kB - 1)) : (ix & (kB - 1));   // x-steps left inside the block
-        int by_left = py ? (kB - 1) - (iy & (kB - 1)) : (iy & (kB - 1));
-        const int bstep_y = py ? bw : -bw;
-        int bcell = (iy >> kBlockShift) * bw + (ix >> kBlockShift);
-        float bm = __ldg(bmax + bcell);
-        for (;;) {
-            const float zr = __fmaf_rn(d.cz, t, oz);
-            if (UP ? (zr > maxz) : (zr < 0.0f)) return 0;
-            if (__fsub_rn(bm, zr) > 0.01f && __fsub_rn(__ldg(grid + cell), zr) > 0.01f) return cell + 1;
-            if (tMaxX < tMaxY) {
-                if (--left_x < 0) return 0;
-                t = tMaxX; cell += sx; tMaxX = __fadd_rn(tMaxX, d.dX);
-                if (--bx_left < 0) { bx_left = kB - 1; bcell += sx; bm = __ldg(bmax + bcell); }
-            } else {
-                if (--left_y < 0) return 0;
-                t = tMaxY; cell += step_y; tMaxY = __fadd_rn(tMaxY, d.dY);
-                if (--by_left < 0) { by_left = kB - 1; bcell += bstep_y; bm = __ldg(bmax + bcell); }
-            }
+    for (;;) {
+        const float zr = __fmaf_rn(d.cz, t, oz);
+        if (UP ? (zr > maxz) : (zr < 0.0f)) return 0;
+        if (__fsub_rn(__ldg(grid + cell), zr) > 0.01f) return cell + 1;
+        if (tMaxX < tMaxY) {
+            if (--left_x < 0) return 0;
+            t = tMaxX; cell += sx; tMaxX = __fadd_rn(tMaxX, d.dX);
+        } else {
+            if (--left_y < 0) return 0;
+            t = tMaxY; cell += step_y; tMaxY = __fadd_rn(tMaxY, d.dY);
         }
     }
 }
 
-__global__ void k_block_max(const float* __restrict__ grid, int W, int H, float* __restrict__ bmax)
-{
-    constexpr int kB = 1 << kBlockShift;
-    const int bw = (W + kB - 1) >> kBlockShift, bh = (H + kB - 1) >> kBlockShift;
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= bw * bh) return;
-    const int x0 = (b % bw) * kB, y0 = (b / bw) * kB;
-    float m = -INFINITY;
-    for (int y = y0; y < min(H, y0 + kB); ++y)
-        for (int x = x0; x < min(W, x0 + kB); ++x) m = fmaxf(m, grid[(size_t)y * W + x]);
-    bmax[b] = m;
-}
-
-template <bool SKIP>
 __global__ void __launch_bounds__(kTraceBlock)
 k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
         int voxel_offset, int chunk_count, int* __restrict__ raw, uint32_t* __restrict__ shadow,
@@ -146,9 +100,8 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
             const DirEntry d = dirs[g0 + k];
             // up/down is the same for the whole warp (one direction at a time)
             const int hit = !active ? 0
-                            : ((d.meta >> 16) & 1)
-                                  ? trace_ray<true, SKIP>(s.grid, s.bmax, s.W, s.H, s.maxz, gx, gy, base_z, d)
-                                  : trace_ray<false, SKIP>(s.grid, s.bmax, s.W, s.H, s.maxz, gx, gy, base_z, d);
+                            : ((d.meta >> 16) & 1) ? trace_ray<true>(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d)
+                                                   : trace_ray<false>(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d);
             stage[k][threadIdx.x] = hit;
             const int dense = (d.meta & 0xFFFF) - 1;   // warp-uniform
             if (dense >= 0) {
@@ -334,24 +287,7 @@ cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int wor
     // D is a multiple of kRawGroup (rows are written kRawGroup directions at a time)
     if (D % kRawGroup != 0) return cudaErrorInvalidValue;
     const dim3 grid((chunk_count + kTraceBlock - 1) / kTraceBlock, kDirParts);
-    if (s.bmax)
-        k_trace<true><<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow, perm);
-    else
-        k_trace<false><<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow, perm);
-    return cudaGetLastError();
-}
-
-size_t block_max_elems(int W, int H)
-{
-    constexpr int kB = 1 << kBlockShift;
-    return (size_t)((W + kB - 1) / kB) * (size_t)((H + kB - 1) / kB);
-}
-
-cudaError_t launch_block_max(const float* grid, int W, int H, float* bmax, cudaStream_t st)
-{
-    const size_t n = block_max_elems(W, H);
-    if (n == 0) return cudaSuccess;
-    k_block_max<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(grid, W, H, bmax);
+    k_trace<<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow, perm);
     return cudaGetLastError();
 }
 
