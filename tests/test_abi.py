@@ -44,7 +44,7 @@ def test_default_options(cuda_lib):
     from solargpu_b200 import api
     o = api.options()
     assert (o.neighbor_format, o.hour_block, o.accumulation, o.reflection) == (0, 256, 0, 0)
-    assert (o.group_size, o.use_graph, o.chunk_voxels) == (64, 1, 0)
+    assert (o.group_size, o.use_graph, o.chunk_voxels) == (128, 1, 0)
 
 
 def test_bad_options_are_rejected_before_device_work(cuda_lib):
