@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--config3-workload", default="dsm4096", help="workload of the config3 block")
     ap.add_argument("--no-config3-plain", action="store_true",
                     help="config3 block without its plain per-hour run (about 5 minutes at 4096 x 4096)")
+    ap.add_argument("--no-config4", action="store_true",
+                    help="skip the 32-tile block (config4 key: one batched graph against tile-by-tile runs)")
     return ap.parse_args()
 
 
@@ -410,6 +412,31 @@ def run_config3(args, ctx, dev, stream, flush) -> dict:
     return res
 
 
+def run_config4(args) -> dict:
+    """32 seeded uneven tiles (sides log-uniform in 128-1024, a site and TMY
+    per tile): every tile in one batch (solar_gpu_run_batch: the hour loops
+    of all tiles as branches of one CUDA graph) against the same tiles run one
+    by one on one context and stream, both on the default path."""
+    import torch
+    from solargpu_b200 import inputs, tiles
+    t0 = time.perf_counter()
+    scenes = [inputs.make_scene(c) for c in tiles.tile_configs(32, seed=0)]
+    gen_s = time.perf_counter() - t0
+    one = tiles.run_tiles(scenes, workers=1)
+    batch = tiles.run_tiles_batched(scenes, runs=3)
+    torch.cuda.synchronize()
+    return {"tiles": len(scenes), "voxels": int(sum(s.num_total for s in scenes)),
+            "host_generation_s": round(gen_s, 2),
+            "tile_by_tile": {"wall_ms": round(one["wall_s"] * 1e3, 1), "voxel_hours_per_s": one["voxel_hours_per_s"],
+                             "how": "one context and stream, solar_gpu_run_device per tile (graph-captured hour "
+                                    "loop each), wall clock around the pass"},
+            "batched": {"ms": batch["batch_ms"], "median_ms": batch["median_ms"],
+                        "voxel_hours_per_s": batch["voxel_hours_per_s"],
+                        "how": "solar_gpu_run_batch: Stage 1 and list builds tile by tile, then every tile's "
+                               "hour loop as a branch of one CUDA graph; CUDA events around the call, median of 3"},
+            "speedup": round(one["wall_s"] * 1e3 / batch["median_ms"], 3)}
+
+
 # ---------------------------------------------------------------- our arm
 
 def run_ours(args, world, rank, local, pg):
@@ -710,10 +737,13 @@ def run_ours(args, world, rank, local, pg):
         nst = min(ns, 2000)
         steps_per_ray = float(O.trace_steps(scene, smp[:nst]).astype(np.float64).mean())
 
-    if rank == 0 and world == 1 and not args.no_config3:
+    if rank == 0 and world == 1 and not (args.no_config3 and args.no_config4):
         del d, out
         ctx.release()
-        extra["config3"] = run_config3(args, ctx, dev, stream, flush)
+        if not args.no_config4:
+            extra["config4"] = run_config4(args)
+        if not args.no_config3:
+            extra["config3"] = run_config3(args, ctx, dev, stream, flush)
         ctx.release()
     if rank == 0:
         line = {

@@ -149,6 +149,19 @@ int solar_gpu_run_device(solar_gpu_context* ctx, const solar_gpu_options* opt,
                          const solar_gpu_scene* scene, float* irradiance_out_device,
                          void* stream);
 
+/* No counterpart in the reference (it runs one DSM per call).  Runs n
+   scenes -- uneven DSM tiles, each with its own site and hourly series -- in
+   n contexts (one per tile, same device, device-resident scenes as for
+   solar_gpu_run_device): Stage 1 and the once-per-run list builds tile by
+   tile, then the hour-block loops of all tiles as parallel branches of one
+   CUDA graph, launched once on `stream` (NULL: the first context's stream),
+   so that the small tiles' persistent reflection kernels share the SMs.
+   opts[i] are tile i's options (e.g. an autotuner's choice for its size)
+   and outs[i] receives its annual irradiance.  Needs hour_block > 1 and
+   hourly reflection; time_kernels is ignored.  Synchronous. */
+int solar_gpu_run_batch(solar_gpu_context* const* ctxs, int n, const solar_gpu_options* opts,
+                        const solar_gpu_scene* scenes, float* const* outs, void* stream);
+
 /* ---- stage access (parity checks, tools) ------------------------------- */
 
 /* Runs Stage 1 only (device scene), building the lists opt->neighbor_format

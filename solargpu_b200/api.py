@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         L.solar_gpu_trace_copy.argtypes = [vp, vp, vp, vp, vp, vp]
         L.solar_gpu_trace_copy_range.argtypes = [vp, i, i, vp, vp, vp, vp, vp]
         L.solar_gpu_run_lists.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), C.POINTER(ListsDesc), vp, vp]
+        L.solar_gpu_run_batch.argtypes = [C.POINTER(vp), i, C.POINTER(Options), C.POINTER(SceneDesc), C.POINTER(vp), vp]
         L.solar_gpu_gemm_bf16.argtypes = [vp, vp, vp, vp, vp, i, i, i, i, vp]
         L.solar_gpu_last_timings.argtypes = [vp, C.POINTER(C.c_double), i]
         L.solar_gpu_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(ll), i]
@@ -176,6 +177,30 @@ def compressed_gpu_irradiance(grid_data, grid_width, grid_height, num_total_voxe
 
 
 # ---------------------------------------------------------------- context
+
+def run_batch(contexts: list, scenes: list, devs: list, outs: list, stream=None, per_tile: list | None = None,
+              **opts) -> None:
+    """Runs many scenes (uneven DSM tiles) at once (solar_gpu_run_batch):
+    Stage 1 and the list builds tile by tile, then every tile's hour-block
+    loop as a branch of one CUDA graph.  One Context per tile; `devs` holds
+    each scene's device arrays (as for Context.run_device), `outs` its
+    device output; `per_tile` optional per-scene option dicts (over `opts`)."""
+    n = len(scenes)
+    if not (len(contexts) == len(devs) == len(outs) == n) or n == 0:
+        raise ValueError("one context, device-array dict and output per scene")
+    o = (Options * n)()
+    for i in range(n):
+        o[i] = options(**dict(opts, **(per_tile[i] if per_tile else {})))
+    descs = (SceneDesc * n)()
+    keep = []
+    for i, (sc, d) in enumerate(zip(scenes, devs)):
+        desc, k = _scene_desc(sc, d)
+        descs[i] = desc
+        keep.append(k)
+    ctx_arr = (C.c_void_p * n)(*[c.h.value for c in contexts])
+    out_arr = (C.c_void_p * n)(*[_p(x) for x in outs])
+    _check(lib().solar_gpu_run_batch(ctx_arr, n, o, descs, out_arr, stream))
+
 
 def gemm_bf16(A, B, out=None, out_bf16=None, bias=None, relu: bool = False, stream=None):
     """C = A @ B.T (+ bias, ReLU) on the tensor cores; A [M, K], B [N, K]

@@ -80,6 +80,26 @@ namespace sgb {
 void set_last_error(const char* msg) { g_err = msg; }
 }  // namespace sgb
 
+// Everything the hour-block loop of one run needs, built by stage23; kept in
+// the context when the loop is enqueued later (solar_gpu_run_batch).
+struct HourLoop {
+    bool mma = false, tiled = false;
+    int group_size = 0, N = 0, T = 0, Hd = 0, B = 0, slab_rows = 0, words32 = 0;
+    sgb::DevGeom g{};
+    const uint32_t* sh = nullptr;
+    const sgb::HourEntry* tab = nullptr;
+    float* slab = nullptr;
+    void* slab16 = nullptr;
+    sgb::MmaLists ml{};
+    sgb::TileLists tl{};
+    sgb::GroupLists gl{};
+    sgb::NeighborLists nl{};
+    sgb::Accum acc{};
+    int* err = nullptr;
+    const int* order = nullptr;
+    float* out = nullptr;
+};
+
 struct solar_gpu_context {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -108,6 +128,9 @@ struct solar_gpu_context {
     // a run released buffers to make room (scenes of tens of millions of
     // voxels): the next run starts by releasing the Stage 2/3 buffers too
     bool squeezed = false;
+    // solar_gpu_run_batch: stage23 stops before the hour loop and leaves it here
+    bool defer_hours = false;
+    HourLoop hours;
     // per kernel-group event log (time_kernels)
     bool ktime = false;
     std::vector<cudaEvent_t> kt_pool;
@@ -475,6 +498,39 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     return SOLAR_GPU_OK;
 }
 
+// The hour-block loop of one run (solar slab + reflection per block of B
+// hours) and the final conversion of the accumulators into the output.
+cudaError_t enqueue_hours(solar_gpu_context* c, const HourLoop& h, cudaStream_t st)
+{
+    cudaError_t le = cudaSuccess;
+    for (int j0 = 0; j0 < h.Hd && le == cudaSuccess; j0 += h.B) {
+        {
+            KScope k(c, SOLAR_GPU_KT_SOLAR);
+            le = h.mma ? launch_solar_slab16(h.g, h.T, h.sh, h.words32, h.tab, j0, h.slab16, st)
+                       : launch_solar_slab(h.g, h.slab_rows, h.sh, h.words32, h.tab, j0, h.B, h.slab, st);
+        }
+        if (le == cudaSuccess) {
+            KScope k(c, SOLAR_GPU_KT_REFLECT);
+            if (h.mma)
+                le = launch_reflect_mma(h.slab16, h.ml, h.g, h.sh, h.words32, h.tab, j0, h.acc, h.err, st);
+            else if (h.tiled)
+                le = launch_reflect_tile(h.B, h.slab, h.tl, h.order, h.acc, h.err, st);
+            else if (h.group_size > 0)
+                le = launch_reflect_group(h.N, h.B, h.slab, h.gl, h.order, h.acc, st);
+            else
+                le = launch_reflect_block(h.g, h.N, h.T, h.sh, h.words32, h.tab, j0, h.B, h.slab, h.nl, h.acc,
+                                          h.order, h.err, st);
+        }
+        c->launches += 2;
+    }
+    if (le == cudaSuccess) {
+        KScope k(c, SOLAR_GPU_KT_FINALIZE);
+        le = launch_finalize(h.acc, h.N, h.out, st);
+        c->launches += 1;
+    }
+    return le;
+}
+
 int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
             const SkyTables& sky, float* out, cudaStream_t st)
 {
@@ -788,31 +844,36 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
             RK(ensure(c, c->slab, sizeof(float) * (size_t)slab_rows * B));
             slab = as<float>(c->slab);
         }
+        HourLoop& h = c->hours;
+        h = HourLoop{};
+        h.mma = mma;
+        h.tiled = tiled;
+        h.group_size = o->group_size;
+        h.N = N;
+        h.T = T;
+        h.Hd = Hd;
+        h.B = B;
+        h.slab_rows = slab_rows;
+        h.words32 = c->words32;
+        h.g = g;
+        h.sh = sh;
+        h.tab = tab;
+        h.slab = slab;
+        h.slab16 = c->slab16.p;
+        h.ml = ml;
+        h.tl = tl;
+        h.gl = gl;
+        h.nl = nl;
+        h.acc = acc;
+        h.err = err;
+        h.order = as<int>(c->order);
+        h.out = out;
+        if (c->defer_hours) return SOLAR_GPU_OK;   // enqueued by solar_gpu_run_batch
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         const bool use_graph = o->use_graph != 0 && !c->ktime;
         if (use_graph) CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        cudaError_t le = cudaSuccess;
-        for (int j0 = 0; j0 < Hd && le == cudaSuccess; j0 += B) {
-            {
-                KScope k(c, SOLAR_GPU_KT_SOLAR);
-                le = mma ? launch_solar_slab16(g, T, sh, c->words32, tab, j0, c->slab16.p, st)
-                         : launch_solar_slab(g, slab_rows, sh, c->words32, tab, j0, B, slab, st);
-            }
-            if (le == cudaSuccess) {
-                KScope k(c, SOLAR_GPU_KT_REFLECT);
-                if (mma)
-                    le = launch_reflect_mma(c->slab16.p, ml, g, sh, c->words32, tab, j0, acc, err, st);
-                else if (tiled)
-                    le = launch_reflect_tile(B, slab, tl, as<int>(c->order), acc, err, st);
-                else if (o->group_size > 0)
-                    le = launch_reflect_group(N, B, slab, gl, as<int>(c->order), acc, st);
-                else
-                    le = launch_reflect_block(g, N, T, sh, c->words32, tab, j0, B, slab, nl, acc,
-                                              as<int>(c->order), err, st);
-            }
-            c->launches += 2;
-        }
+        cudaError_t le = enqueue_hours(c, h, st);
         if (use_graph) {
             const cudaError_t ce = cudaStreamEndCapture(st, &graph);
             if (le == cudaSuccess) le = ce;
@@ -822,6 +883,7 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
             if (graph) cudaGraphDestroy(graph);
         }
         CK(le);
+        return SOLAR_GPU_OK;
     }
     {
         KScope k(c, SOLAR_GPU_KT_FINALIZE);
@@ -1141,6 +1203,68 @@ int solar_gpu_run_device(solar_gpu_context* c, const solar_gpu_options* o, const
     cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
     RK(run_device_impl(c, o, s, out, st, false));
     return check_device_flags(c, st);
+}
+
+int solar_gpu_run_batch(solar_gpu_context* const* ctxs, int n, const solar_gpu_options* opts,
+                        const solar_gpu_scene* scenes, float* const* outs, void* stream)
+{
+    if (!ctxs || !scenes || !outs || !opts || n <= 0) return fail(SOLAR_GPU_ERR_ARG, "NULL argument or n <= 0");
+    for (int i = 0; i < n; ++i) {
+        if (!ctxs[i] || !outs[i]) return fail(SOLAR_GPU_ERR_ARG, "context or output %d is NULL", i);
+        if (ctxs[i]->device != ctxs[0]->device) return fail(SOLAR_GPU_ERR_ARG, "contexts on different devices");
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i]) return fail(SOLAR_GPU_ERR_ARG, "context %d is given twice", i);
+    }
+    for (int i = 0; i < n; ++i)
+        if (opts[i].hour_block == 1 || opts[i].reflection != SOLAR_GPU_REFL_HOURLY)
+            return fail(SOLAR_GPU_ERR_ARG, "a batch runs the hour-block path (hour_block > 1, hourly reflection)");
+    CK(cudaSetDevice(ctxs[0]->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctxs[0]->own;
+    // Stage 1 and the once-per-run builds, tile after tile (each sizes its
+    // buffers from its own lists); each stops before its hour loop.
+    for (int i = 0; i < n; ++i) {
+        solar_gpu_context* c = ctxs[i];
+        solar_gpu_options ob = opts[i];
+        ob.time_kernels = 0;
+        c->defer_hours = true;
+        const int rc = run_device_impl(c, &ob, &scenes[i], outs[i], st, false);
+        c->defer_hours = false;
+        if (rc != SOLAR_GPU_OK) return rc;
+    }
+    // One CUDA graph holds every tile's hour loop as a branch of its own (on
+    // the tile context's stream, forked from and joined back into `st`), so
+    // the small tiles' persistent kernels run side by side on the SMs.
+    std::vector<cudaEvent_t> ev(n + 1, nullptr);
+    cudaError_t le = cudaSuccess;
+    for (int i = 0; i <= n && le == cudaSuccess; ++i) le = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool capturing = false;
+    if (le == cudaSuccess) le = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (le == cudaSuccess) {
+        capturing = true;
+        le = cudaEventRecord(ev[n], st);
+    }
+    for (int i = 0; i < n && le == cudaSuccess; ++i) {
+        solar_gpu_context* c = ctxs[i];
+        le = cudaStreamWaitEvent(c->own, ev[n], 0);
+        if (le == cudaSuccess) le = enqueue_hours(c, c->hours, c->own);
+        if (le == cudaSuccess) le = cudaEventRecord(ev[i], c->own);
+        if (le == cudaSuccess) le = cudaStreamWaitEvent(st, ev[i], 0);
+    }
+    if (capturing) {
+        const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        if (le == cudaSuccess) le = ce;
+    }
+    if (le == cudaSuccess) le = cudaGraphInstantiate(&exec, graph, 0);
+    if (le == cudaSuccess) le = cudaGraphLaunch(exec, st);
+    if (le == cudaSuccess) le = cudaStreamSynchronize(st);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
+    CK(le);
+    for (int i = 0; i < n; ++i) RK(check_device_flags(ctxs[i], st));
+    return SOLAR_GPU_OK;
 }
 
 int solar_gpu_run_lists(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,

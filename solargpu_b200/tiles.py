@@ -11,7 +11,9 @@ Tiles are generated on the host and uploaded once; each run is one
 
 Worker threads each own a context and a CUDA stream, so the small tiles of
 one worker overlap the host-side set-up and launches of another (the ctypes
-calls release the GIL).  The autotuner times each candidate configuration
+calls release the GIL).  `--batch` also runs all tiles through
+solar_gpu_run_batch: Stage 1 and the list builds tile by tile, then the
+hour-block loops of every tile as branches of one CUDA graph, launched once.  The autotuner times each candidate configuration
 (list format x hour block x reflection kernel) on the first tile of a size
 bucket (log2 of the voxel count), alone on the GPU before the workers start,
 and reuses the fastest for the bucket; the table can be saved and reloaded
@@ -195,6 +197,53 @@ def run_tiles(scenes: list, params: dict | None = None, tuner: Autotuner | None 
             "sum_tile_ms": sum(r["ms"] for r in results)}
 
 
+def run_tiles_batched(scenes: list, params: dict | None = None, tuner: Autotuner | None = None, device: int = 0,
+                      accumulation: int = 1, runs: int = 2, keep_outputs: bool = False) -> dict:
+    """Every tile in one batch (solar_gpu_run_batch): one context per tile,
+    Stage 1 and the list builds tile by tile, then all hour-block loops as
+    branches of one CUDA graph.  One untimed batch sizes the buffers; the
+    median of `runs` timed batches (CUDA events around the call) is
+    reported.  With a tuner, each tile runs the configuration its size bucket
+    was tuned to (tune first, e.g. with run_tiles)."""
+    import torch
+    from . import api
+
+    dev = torch.device("cuda", device)
+    torch.cuda.set_device(dev)
+    devs = [_device_arrays(s, dev) for s in scenes]
+    outs = [torch.empty(s.num_total, dtype=torch.float32, device=dev) for s in scenes]
+    per_tile = []
+    for s in scenes:
+        p = dict(params or DEFAULT)
+        if tuner is not None and size_bucket(s) in tuner.table:
+            p = dict(tuner.table[size_bucket(s)])
+        p["accumulation"] = accumulation
+        per_tile.append(p)
+    ctxs = [api.Context(device) for _ in scenes]
+    stream = torch.cuda.Stream(device=dev)
+    try:
+        api.run_batch(ctxs, scenes, devs, outs, stream=stream.cuda_stream, per_tile=per_tile)
+        ms = []
+        for _ in range(max(1, runs)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            api.run_batch(ctxs, scenes, devs, outs, stream=stream.cuda_stream, per_tile=per_tile)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    finally:
+        for c in ctxs:
+            c.close()
+    vh = float(sum(s.num_total * int(((s.sun[:, 1] - np.float32(1e-8)) >= 1.0).sum()) for s in scenes))
+    t = sorted(ms)[len(ms) // 2]
+    r = {"batch_ms": [round(x, 2) for x in ms], "median_ms": round(t, 2), "voxel_hours": vh,
+         "voxel_hours_per_s": vh / (t / 1e3), "params": per_tile}
+    if keep_outputs:
+        r["outs"] = [o.cpu().numpy() for o in outs]
+    return r
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--tiles", type=int, default=32)
@@ -202,6 +251,8 @@ def main(argv=None) -> int:
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--tune", action="store_true", help="autotune per size bucket (else the default path)")
     ap.add_argument("--table", default=None, help="autotuner table (JSON) to load and update")
+    ap.add_argument("--batch", action="store_true",
+                    help="also run every tile in one batch (one CUDA graph over all hour loops)")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
     scenes = [inputs.make_scene(c) for c in tile_configs(a.tiles, a.seed)]
@@ -212,6 +263,9 @@ def main(argv=None) -> int:
     r["workers"] = a.workers
     if tuner is not None:
         r["autotuner"] = {str(k): {"chosen": v, "trials_ms": tuner.trials.get(k)} for k, v in tuner.table.items()}
+    if a.batch:
+        b = run_tiles_batched(scenes, tuner=tuner)
+        r["batched"] = {k: v for k, v in b.items() if k != "params"}
     print(json.dumps(r))
     return 0
 
