@@ -111,7 +111,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -139,7 +139,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 74;
+static constexpr int kNumBufs = 75;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -394,6 +394,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     CK(cudaMemsetAsync(c->shadow.p, 0, sizeof(uint32_t) * (size_t)N * c->words32, st));
     RK(ensure(c, c->raw, sizeof(int) * (size_t)chunk * D));
     RK(ensure(c, c->counts, sizeof(int) * (size_t)N));
+    RK(ensure(c, c->dd_ovf, sizeof(int) * ((size_t)chunk + 1)));
     RK(ensure(c, c->scan_tmp, sizeof(long long) * scan_scratch_elems((int)chunk)));
     if (want_csr) {
         RK(ensure(c, c->csr_off, sizeof(long long) * ((size_t)N + 1)));
@@ -442,7 +443,8 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         }
         {
             KScope k(c, SOLAR_GPU_KT_DEDUPE);
-            CK(launch_dedupe(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->err), perm, st));
+            CK(launch_dedupe(n, D, as<int>(c->raw), as<int>(c->counts) + v0, as<int>(c->err), perm,
+                             as<int>(c->dd_ovf), st));
         }
         c->launches += 2;
         const double frac_left = (double)N / (double)(v0 + n);
@@ -1145,7 +1147,8 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_rows, &c->tile_gcnt, &c->tile_gnch, &c->tile_gbase, &c->tile_tbase,
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
-                                &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16};
+                                &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
+                                &c->dd_ovf};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

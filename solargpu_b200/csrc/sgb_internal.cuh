@@ -73,7 +73,8 @@ void set_last_error(const char* msg);
 cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
                          int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
                          const int* perm, cudaStream_t st);
-cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, const int* perm,
+// ovf: chunk_count + 1 ints of scratch (rows the small-table pass hands on).
+cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, const int* perm, int* ovf,
                           cudaStream_t st);
 cudaError_t launch_invert(const int* perm, int n, int* inv, cudaStream_t st);
 // perm = the chunk voxels [v0, v0 + n) (as v - v0) in visiting order;

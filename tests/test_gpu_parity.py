@@ -48,6 +48,30 @@ def test_trace_matches_oracle(ctx, name):
     np.testing.assert_array_equal(r["barle"], buf)
 
 
+def test_dedupe_second_pass_gives_the_same_lists(cuda_lib, scene160):
+    """The first-occurrence dedupe first runs with small hash sets and hands
+    the rows it gives up on to a second pass with large ones.  With the
+    first pass's probe bound forced down to one probe (SGB_DEDUPE_PROBES=1)
+    most rows take the second pass, after part of them was already compacted:
+    the lists must still equal the oracle's.  Runs in a child process so the
+    setting stays out of the other tests."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, 'tests'); sys.path.insert(0, '.');"
+        "from conftest import load_scene, device_arrays, oracle_trace;"
+        "from solargpu_b200 import api;"
+        "s = load_scene('dsm160'); bins, off, ids, sh = oracle_trace(s);"
+        "c = api.Context(0); r = c.trace(s, device_arrays(s), neighbor_format=0);"
+        "assert np.array_equal(r['csr_off'], off) and np.array_equal(r['csr_ids'], ids);"
+        "assert np.array_equal(r['shadow'], sh); print('same lists')")
+    env = dict(os.environ, SGB_DEDUPE_PROBES="1")
+    p = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0 and "same lists" in p.stdout, p.stdout + p.stderr
+
+
 def test_trace_chunked_equals_single(ctx, scene160):
     dev = device_arrays(scene160)
     a = ctx.trace(scene160, dev)
