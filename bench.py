@@ -720,6 +720,28 @@ def run_ours(args, world, rank, local, pg):
                                   "oracle": "FP64 annual-sum form over every voxel, on the GPU-built neighbor lists "
                                             "and shadow bits (those are checked by list_parity on the sample)"}
         del r
+    if rank == 0:
+        # caller-side voxelization of the heightmap: the reference's host
+        # restatement (numpy) against solar_gpu_voxelize, same arrays
+        heights = scene.grid.reshape(scene.height, scene.width)
+        t0 = time.perf_counter()
+        inputs.voxelize(heights, 1.0)
+        host_s = time.perf_counter() - t0
+        g = torch.from_numpy(scene.grid).to(dev)
+        ctx.voxelize(g, scene.width, scene.height, 1.0)   # warm (buffers)
+        torch.cuda.synchronize(dev)
+        gms = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            v = ctx.voxelize(g, scene.width, scene.height, 1.0)
+            torch.cuda.synchronize(dev)
+            gms.append((time.perf_counter() - t0) * 1e3)
+        same = bool(torch.equal(v["pixel_parent"].cpu(), torch.from_numpy(scene.pixel_parent)))
+        extra["voxelize"] = {"gpu_ms": round(sorted(gms)[1], 3), "host_numpy_ms": round(host_s * 1e3, 1),
+                             "voxels": v["num_total"], "pixel_parent_equal": same,
+                             "how": "solar_gpu_voxelize (count, scan, write; wall clock around the synchronous "
+                                    "call, median of 3) against the numpy restatement of src/voxelization.cpp"}
+        del g, v
     cpu = None
     steps_per_ray = nst = None
     if rank == 0 and world == 1 and not args.no_cpu:

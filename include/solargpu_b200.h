@@ -162,6 +162,23 @@ int solar_gpu_run_device(solar_gpu_context* ctx, const solar_gpu_options* opt,
 int solar_gpu_run_batch(solar_gpu_context* const* ctxs, int n, const solar_gpu_options* opts,
                         const solar_gpu_scene* scenes, float* const* outs, void* stream);
 
+/* Voxelization of a heightmap on the GPU, replacing the reference's host
+   code (src/voxelization.cpp:10-97, detect_wall_voxels and
+   compute_top_slope_aspect, packed as src/main.cpp:112-127 packs them): one
+   top voxel per cell in raster order (pixel_parent i = i, slope and aspect
+   from central differences over cells of voxel_size), then the column-drop
+   wall voxels in raster order of their cell, from the top of the drop
+   downwards (wall_z, slope pi/2, aspect from the open sides).  grid is a
+   device array [H][W]; *num_total (host) receives T + walls.  With all
+   output pointers NULL only the count is made; otherwise pixel_parent,
+   slopes, aspects are device arrays of capacity >= *num_total voxels and
+   wall_z of *num_total - T (may be NULL without walls).  Wall counts and
+   heights are identical to the reference's; angles may differ from the host
+   library's atan2f in the last bits.  Synchronous on `stream`. */
+int solar_gpu_voxelize(solar_gpu_context* ctx, const float* grid, int W, int H, float voxel_size,
+                       long long* num_total, int* pixel_parent, float* wall_z, float* slopes, float* aspects,
+                       long long capacity, void* stream);
+
 /* ---- stage access (parity checks, tools) ------------------------------- */
 
 /* Runs Stage 1 only (device scene), building the lists opt->neighbor_format

@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         L.solar_gpu_trace_copy.argtypes = [vp, vp, vp, vp, vp, vp]
         L.solar_gpu_trace_copy_range.argtypes = [vp, i, i, vp, vp, vp, vp, vp]
         L.solar_gpu_run_lists.argtypes = [vp, C.POINTER(Options), C.POINTER(SceneDesc), C.POINTER(ListsDesc), vp, vp]
+        L.solar_gpu_voxelize.argtypes = [vp, vp, i, i, f, C.POINTER(ll), vp, vp, vp, vp, ll, vp]
         L.solar_gpu_run_batch.argtypes = [C.POINTER(vp), i, C.POINTER(Options), C.POINTER(SceneDesc), C.POINTER(vp), vp]
         L.solar_gpu_gemm_bf16.argtypes = [vp, vp, vp, vp, vp, i, i, i, i, vp]
         L.solar_gpu_last_timings.argtypes = [vp, C.POINTER(C.c_double), i]
@@ -308,6 +309,27 @@ class Context:
         ld = ListsDesc(fmt, _p(off), _p(data) if data.size else None, int(data.size), _p(shadow),
                        int(lists["shadow_words"]), int(lists["active_bins"]))
         _check(lib().solar_gpu_run_lists(self.h, C.byref(o), C.byref(d), C.byref(ld), _p(out), stream))
+
+    def voxelize(self, grid, width: int, height: int, voxel_size: float = 1.0, stream=None) -> dict:
+        """Voxelizes a device heightmap (torch tensor [H*W] float32) on the GPU
+        (solar_gpu_voxelize); returns device tensors pixel_parent, wall_z,
+        slopes, aspects and the counts, packed as the drop-in entry points take
+        them."""
+        import torch
+        n = C.c_longlong()
+        _check(lib().solar_gpu_voxelize(self.h, _p(grid), width, height, float(voxel_size), C.byref(n), None, None,
+                                        None, None, 0, stream))
+        N, T = int(n.value), width * height
+        dev = grid.device
+        out = {"pixel_parent": torch.empty(N, dtype=torch.int32, device=dev),
+               "wall_z": torch.empty(max(1, N - T), dtype=torch.float32, device=dev),
+               "slopes": torch.empty(N, dtype=torch.float32, device=dev),
+               "aspects": torch.empty(N, dtype=torch.float32, device=dev)}
+        _check(lib().solar_gpu_voxelize(self.h, _p(grid), width, height, float(voxel_size), C.byref(n),
+                                        _p(out["pixel_parent"]), _p(out["wall_z"]), _p(out["slopes"]),
+                                        _p(out["aspects"]), N, stream))
+        out["num_total"], out["num_top"] = N, T
+        return out
 
     def stage1(self, scene, dev: dict, neighbor_format: int = BOTH, stream=None, **opts) -> None:
         """Runs Stage 1 only and keeps its products on the device (read them

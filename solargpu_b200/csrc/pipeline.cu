@@ -111,7 +111,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -139,7 +139,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 75;
+static constexpr int kNumBufs = 78;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -1148,7 +1148,7 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
                                 &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
-                                &c->dd_ovf};
+                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 
@@ -1267,6 +1267,37 @@ int solar_gpu_run_batch(solar_gpu_context* const* ctxs, int n, const solar_gpu_o
     for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
     CK(le);
     for (int i = 0; i < n; ++i) RK(check_device_flags(ctxs[i], st));
+    return SOLAR_GPU_OK;
+}
+
+int solar_gpu_voxelize(solar_gpu_context* c, const float* grid, int W, int H, float voxel_size,
+                       long long* num_total, int* pixel_parent, float* wall_z, float* slopes, float* aspects,
+                       long long capacity, void* stream)
+{
+    if (!c || !grid || !num_total) return fail(SOLAR_GPU_ERR_ARG, "context, grid or num_total is NULL");
+    if (W <= 0 || H <= 0 || (long long)W * H > 0x7FFFFFFFLL) return fail(SOLAR_GPU_ERR_ARG, "grid %d x %d", W, H);
+    if (!(voxel_size > 0.0f)) return fail(SOLAR_GPU_ERR_ARG, "voxel_size must be > 0");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->own;
+    const int T = W * H;
+    RK(ensure(c, c->vox_cnt, sizeof(int) * (size_t)T));
+    RK(ensure(c, c->vox_off, sizeof(long long) * ((size_t)T + 1)));
+    RK(ensure(c, c->vox_tmp, sizeof(long long) * scan_scratch_elems(T)));
+    CK(launch_vox_count(grid, W, H, voxel_size, as<int>(c->vox_cnt), st));
+    CK(launch_scan_counts(as<int>(c->vox_cnt), T, 0, as<long long>(c->vox_off), as<long long>(c->vox_tmp), nullptr,
+                          st));
+    long long walls = 0;
+    RK(read_ll(c, as<long long>(c->vox_off) + T, &walls, st));
+    *num_total = (long long)T + walls;
+    if (!pixel_parent && !slopes && !aspects) return SOLAR_GPU_OK;   // sizes only
+    if (!pixel_parent || !slopes || !aspects || (walls > 0 && !wall_z))
+        return fail(SOLAR_GPU_ERR_ARG, "an output array is NULL");
+    if (capacity < *num_total) return fail(SOLAR_GPU_ERR_ARG, "capacity %lld < %lld voxels", capacity, *num_total);
+    if (*num_total > 0x7FFFFFFFLL) return fail(SOLAR_GPU_ERR_ARG, "%lld voxels exceed the int32 voxel index", *num_total);
+    // the cell size of the slope differences is the voxel size (src/main.cpp:103)
+    CK(launch_vox_write(grid, W, H, voxel_size, voxel_size, as<long long>(c->vox_off), pixel_parent, wall_z, slopes,
+                        aspects, st));
+    CK(cudaStreamSynchronize(st));
     return SOLAR_GPU_OK;
 }
 

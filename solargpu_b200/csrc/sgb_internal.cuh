@@ -236,4 +236,10 @@ cudaError_t launch_reflect_mma(const void* slab16, const MmaLists& ml, const Dev
                                int words32, const HourEntry* table, int j0, const Accum& acc, int* err,
                                cudaStream_t st);
 
+// voxelization (voxel.cu): wall voxels per cell, then the packed arrays
+// (tops [0, T), walls after them at T + off[cell] + v).
+cudaError_t launch_vox_count(const float* grid, int W, int H, float voxel_size, int* counts, cudaStream_t st);
+cudaError_t launch_vox_write(const float* grid, int W, int H, float voxel_size, float scale, const long long* off,
+                             int* parent, float* wall_z, float* slopes, float* aspects, cudaStream_t st);
+
 }  // namespace sgb
