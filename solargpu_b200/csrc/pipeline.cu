@@ -111,7 +111,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp, gpad;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -139,7 +139,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 78;
+static constexpr int kNumBufs = 79;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -238,6 +238,10 @@ int check_scene(const solar_gpu_scene* s)
         return fail(SOLAR_GPU_ERR_ARG, "grid size %dx%d", s->grid_width, s->grid_height);
     if ((long long)s->grid_width * s->grid_height != (long long)s->num_top_voxels)
         return fail(SOLAR_GPU_ERR_ARG, "num_top_voxels %d != grid_width * grid_height", s->num_top_voxels);
+    // the tracer's bordered copy of the grid is indexed with int
+    if ((long long)(s->grid_width + 2) * (s->grid_height + 2) > 0x7FFFFFFFLL)
+        return fail(SOLAR_GPU_ERR_ARG, "grid %dx%d: (width + 2) * (height + 2) must stay below 2^31",
+                    s->grid_width, s->grid_height);
     if (s->num_total_voxels < s->num_top_voxels)
         return fail(SOLAR_GPU_ERR_ARG, "num_total_voxels %d < num_top_voxels", s->num_total_voxels);
     if (!s->grid || !s->pixel_parent || !s->slopes || !s->aspects)
@@ -282,6 +286,7 @@ DevScene dev_scene(const solar_gpu_scene* s)
 {
     DevScene d;
     d.grid = s->grid;
+    d.gpad = nullptr;
     d.pix_parent = s->pixel_parent;
     d.wall_z = s->wall_z;
     d.slopes = s->slopes;
@@ -377,6 +382,17 @@ long long auto_chunk(solar_gpu_context* c, int N, int D)
     return chunk;
 }
 
+// The tracer's copy of the heightmap inside a border of +inf (one pass over
+// the grid, rebuilt each call: the caller may change heights between calls).
+int padded_grid(solar_gpu_context* c, const solar_gpu_scene* s, DevScene& ds, cudaStream_t st)
+{
+    RK(ensure(c, c->gpad, sizeof(float) * (size_t)(s->grid_width + 2) * (size_t)(s->grid_height + 2)));
+    CK(launch_pad_grid(s->grid, s->grid_width, s->grid_height, as<float>(c->gpad), st));
+    c->launches += 1;
+    ds.gpad = as<float>(c->gpad);
+    return SOLAR_GPU_OK;
+}
+
 int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_scene* s,
            const SkyTables& sky, cudaStream_t st, bool want_csr, bool want_barle)
 {
@@ -405,7 +421,8 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         RK(ensure(c, c->barle_sizes, sizeof(int) * (size_t)N));
         RK(ensure(c, c->barle_bytes, (size_t)N * 160));
     }
-    const DevScene ds = dev_scene(s);
+    DevScene ds = dev_scene(s);
+    RK(padded_grid(c, s, ds, st));
     // Rows follow the visiting order (Morton-adjacent voxels share a warp, so
     // their rays have similar lengths); with several chunks, each chunk (a
     // range of voxel indices) is traced in the visiting order of its voxels.
@@ -439,7 +456,7 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         {
             KScope k(c, SOLAR_GPU_KT_TRACE);
             CK(launch_trace(ds, as<DirEntry>(c->dirs), D, c->words32, (int)v0, n, as<int>(c->raw),
-                            as<uint32_t>(c->shadow), perm, st));
+                            as<uint32_t>(c->shadow), perm, as<int>(c->err), st));
         }
         {
             KScope k(c, SOLAR_GPU_KT_DEDUPE);
@@ -901,7 +918,7 @@ int check_device_flags(solar_gpu_context* c, cudaStream_t st)
     CK(cudaStreamSynchronize(st));
     int f = 0;
     std::memcpy(&f, c->h_scalars, sizeof(int));
-    if (f) return fail(SOLAR_GPU_ERR_DEVICE_CHECK, "device check flags 0x%x (1 = ba-RLE stream, 2 = hash, 4 = capacity, 8 = wait timeout)", f);
+    if (f) return fail(SOLAR_GPU_ERR_DEVICE_CHECK, "device check flags 0x%x (1 = ba-RLE stream, 2 = hash, 4 = capacity, 8 = wait timeout, 16 = tracer border)", f);
     return SOLAR_GPU_OK;
 }
 
@@ -1048,13 +1065,14 @@ int trace_subset_impl(solar_gpu_context* c, const solar_gpu_scene* s, const int*
     int bad = 0;
     std::memcpy(&bad, c->h_scalars, sizeof(int));
     if (bad) return fail(SOLAR_GPU_ERR_ARG, "voxel ids outside [0, %d)", N);
-    CK(launch_trace(dev_scene(s), as<DirEntry>(c->dirs), D, words32, 0, n, as<int>(c->raw),
-                    as<uint32_t>(c->shadow), voxels, st));
+    DevScene ds = dev_scene(s);
+    RK(padded_grid(c, s, ds, st));
+    CK(launch_trace(ds, as<DirEntry>(c->dirs), D, words32, 0, n, as<int>(c->raw),
+                    as<uint32_t>(c->shadow), voxels, as<int>(c->err), st));
     const long long cells = (long long)n * words32;
     k_gather_shadow<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(as<uint32_t>(c->shadow), words32, voxels, n, out);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(st));
-    return SOLAR_GPU_OK;
+    return check_device_flags(c, st);
 }
 
 std::mutex g_default_mu;
@@ -1148,7 +1166,7 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
                                 &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
-                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp};
+                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp, &c->gpad};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

@@ -19,6 +19,7 @@ enum DeviceError : int {
     kErrHashFull = 2,      // a dedupe hash probe exceeded its bound
     kErrListCapacity = 4,  // a neighbor list exceeded the buffer capacity
     kErrWaitTimeout = 8,   // a bounded wait on a shared-memory barrier expired
+    kErrTraceBounds = 16,  // a ray passed the tracer's border (the index check ended it)
 };
 
 // One traced direction; host-computed exactly as the reference computes Cdir
@@ -44,6 +45,7 @@ struct HourEntry {
 
 struct DevScene {
     const float* grid;        // [T]
+    const float* gpad;        // [H + 2][W + 2]: grid inside a border of +inf (the tracer's copy)
     const int* pix_parent;    // [N]
     const float* wall_z;      // [N - T] or nullptr
     const float* slopes;      // [N]
@@ -70,9 +72,12 @@ void set_last_error(const char* msg);
 // [voxel_offset, voxel_offset + chunk_count).  Row lv holds chunk voxel
 // perm[lv] when a permutation is given (counts, sizes indexed by chunk
 // voxel), else chunk voxel lv; kernels that iterate voxels take the inverse.
+// gpad [(H + 2) * (W + 2)] = grid inside a one-cell border of +inf.
+cudaError_t launch_pad_grid(const float* grid, int W, int H, float* gpad, cudaStream_t st);
+// s.gpad must be set (launch_pad_grid).
 cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
                          int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
-                         const int* perm, cudaStream_t st);
+                         const int* perm, int* err, cudaStream_t st);
 // ovf: chunk_count + 1 ints of scratch (rows the small-table pass hands on).
 cudaError_t launch_dedupe(int chunk_count, int D, int* raw, int* counts, int* err, const int* perm, int* ovf,
                           cudaStream_t st);

@@ -32,8 +32,16 @@ constexpr int kDedupeWarps = 4;
 constexpr int kHashSlots = 4096;   // > 2592 possible distinct hits per voxel
 constexpr int kDedupeBatch = 9;    // 2592 = 9 batches of 9 rounds of 32 directions
 
+// The tracer reads the heightmap from a copy with a one-cell border of +inf
+// ([H + 2][W + 2], cell (x, y) at (x + 1) + (y + 1) * (W + 2)).  A ray that
+// steps off the grid meets the border, whose height test is always true, so
+// the loop needs no per-axis step counts; the cell it stopped on tells a
+// border stop (no hit, as the reference's bounds check) from a hit.  Heights
+// inside the grid are the caller's, +inf included.  One unsigned compare a
+// step keeps every load inside the copy whatever the float tests do; it
+// never ends a ray (the border does first) and returns -1 if it did.
 template <bool UP>
-__device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, int H, float maxz, int gx, int gy,
+__device__ __forceinline__ int trace_ray(const float* __restrict__ gpad, int W, int H, float maxz, int gx, int gy,
                                          float base_z, const DirEntry& d)
 {
     // Cdir * 2.0f is exact, so these match the reference fused or not.
@@ -49,34 +57,40 @@ __device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, 
     const int sx = px ? 1 : -1;
     const int sy = py ? 1 : -1;
     // The first step checks both coordinates (the start cell, never tested,
-    // may lie outside the grid); after it the ray is inside, and each later
-    // step checks only the coordinate it moves, by counting the steps left
-    // on that axis.  Each step moves one cell in a fixed direction, so the
-    // loop leaves the grid after at most W + H steps.
+    // may lie up to two cells outside the grid); after it the ray is inside
+    // and moves one cell a step, so it stops on the border at the latest.
     float t;
     if (tMaxX < tMaxY) { t = tMaxX; ix += sx; tMaxX = __fadd_rn(tMaxX, d.dX); }
     else               { t = tMaxY; iy += sy; tMaxY = __fadd_rn(tMaxY, d.dY); }
     if ((unsigned)ix >= (unsigned)W || (unsigned)iy >= (unsigned)H) return 0;
-    int left_x = px ? W - 1 - ix : ix;
-    int left_y = py ? H - 1 - iy : iy;
-    const int step_y = py ? W : -W;
-    int cell = ix + iy * W;
+    // A start height of NaN or +inf gives no hit in the reference (every test
+    // on it is false, or true only for the height range); it would also keep
+    // the border test false, so it ends here.  -inf still stops on the border.
+    if (oz != oz || oz == __int_as_float(0x7f800000)) return 0;
+    const int Wp = W + 2;
+    const int step_y = py ? Wp : -Wp;
+    int cell = (ix + 1) + (iy + 1) * Wp;
+    const unsigned cells = (unsigned)Wp * (unsigned)(H + 2);
+    float zr;
     for (;;) {
-        const float zr = __fmaf_rn(d.cz, t, oz);
-        if (UP ? (zr > maxz) : (zr < 0.0f)) return 0;
-        if (__fsub_rn(__ldg(grid + cell), zr) > 0.01f) return cell + 1;
+        if ((unsigned)cell >= cells) return -1;
+        zr = __fmaf_rn(d.cz, t, oz);
+        // the reference tests the height range before the hit; both end the
+        // ray, and which one it was is decided once, after the loop
+        if ((UP ? (zr > maxz) : (zr < 0.0f)) || __fsub_rn(__ldg(gpad + cell), zr) > 0.01f) break;
         // one step, as selects: lanes that step on different axes stay
         // converged (measured 119.6 -> 116.5 ms at 1024^2 against branches)
         const bool xs = tMaxX < tMaxY;
-        if ((xs ? left_x : left_y) <= 0) return 0;
-        left_x -= xs ? 1 : 0;
-        left_y -= xs ? 0 : 1;
-        t = xs ? tMaxX : tMaxY;
+        t = fminf(tMaxX, tMaxY);   // = xs ? tMaxX : tMaxY (equal when not xs and equal)
         cell += xs ? sx : step_y;
         const float nx = __fadd_rn(tMaxX, d.dX), ny = __fadd_rn(tMaxY, d.dY);
         tMaxX = xs ? nx : tMaxX;
         tMaxY = xs ? tMaxY : ny;
     }
+    if (UP ? (zr > maxz) : (zr < 0.0f)) return 0;
+    const int r = cell / Wp, q = cell - r * Wp;
+    if (q == 0 || q > W || r == 0 || r > H) return 0;   // the border: the ray left the grid
+    return (q - 1) + (r - 1) * W + 1;
 }
 
 // 16 blocks of 128 threads per SM: at most 32 registers a thread, so the SM
@@ -85,7 +99,7 @@ __device__ __forceinline__ int trace_ray(const float* __restrict__ grid, int W, 
 __global__ void __launch_bounds__(kTraceBlock, 16)
 k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
         int voxel_offset, int chunk_count, int* __restrict__ raw, uint32_t* __restrict__ shadow,
-        const int* __restrict__ perm)
+        const int* __restrict__ perm, int* __restrict__ err)
 {
     __shared__ int stage[kRawGroup][kTraceBlock];
     const int lv = blockIdx.x * kTraceBlock + threadIdx.x;
@@ -109,9 +123,13 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
         for (int k = 0; k < kRawGroup; ++k) {
             const DirEntry d = dirs[g0 + k];
             // up/down is the same for the whole warp (one direction at a time)
-            const int hit = !active ? 0
-                            : ((d.meta >> 16) & 1) ? trace_ray<true>(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d)
-                                                   : trace_ray<false>(s.grid, s.W, s.H, s.maxz, gx, gy, base_z, d);
+            int hit = !active ? 0
+                      : ((d.meta >> 16) & 1) ? trace_ray<true>(s.gpad, s.W, s.H, s.maxz, gx, gy, base_z, d)
+                                             : trace_ray<false>(s.gpad, s.W, s.H, s.maxz, gx, gy, base_z, d);
+            if (hit < 0) {
+                atomicOr(err, kErrTraceBounds);
+                hit = 0;
+            }
             stage[k][threadIdx.x] = hit;
             const int dense = (d.meta & 0xFFFF) - 1;   // warp-uniform
             if (dense >= 0) {
@@ -134,6 +152,18 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
         }
     }
     if (active && acc && cur_word >= 0) atomicOr(shadow + (size_t)v * words32 + cur_word, acc);
+}
+
+__global__ void k_pad_grid(const float* __restrict__ grid, int W, int H, float* __restrict__ gpad)
+{
+    const int Wp = W + 2;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)Wp * (H + 2)) return;
+    const int x = (int)(i % Wp) - 1, y = (int)(i / Wp) - 1;
+    // the load is clamped into the grid, so it stays in bounds however the
+    // select below is compiled
+    const float h = grid[(size_t)min(max(y, 0), H - 1) * W + min(max(x, 0), W - 1)];
+    gpad[i] = (x >= 0 && x < W && y >= 0 && y < H) ? h : __int_as_float(0x7f800000);
 }
 
 __device__ __forceinline__ uint32_t hash_slot(uint32_t x, int bits)
@@ -321,15 +351,24 @@ k_gather_csr(int chunk_count, int D, const int* __restrict__ raw, const long lon
 
 }  // namespace
 
+cudaError_t launch_pad_grid(const float* grid, int W, int H, float* gpad, cudaStream_t st)
+{
+    const long long n = (long long)(W + 2) * (H + 2);
+    if (n <= 0) return cudaSuccess;
+    k_pad_grid<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(grid, W, H, gpad);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
                          int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
-                         const int* perm, cudaStream_t st)
+                         const int* perm, int* err, cudaStream_t st)
 {
     if (chunk_count <= 0) return cudaSuccess;
+    if (!s.gpad) return cudaErrorInvalidValue;
     // D is a multiple of kRawGroup (rows are written kRawGroup directions at a time)
     if (D % kRawGroup != 0) return cudaErrorInvalidValue;
     const dim3 grid((chunk_count + kTraceBlock - 1) / kTraceBlock, kDirParts);
-    k_trace<<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow, perm);
+    k_trace<<<grid, kTraceBlock, 0, st>>>(s, dirs, D, words32, voxel_offset, chunk_count, raw, shadow, perm, err);
     return cudaGetLastError();
 }
 

@@ -25,7 +25,9 @@ constexpr float kPiF = 3.14159265358979323846f;
 
 __device__ __forceinline__ float height_at(const float* g, int W, int H, int x, int y)
 {
-    return (x >= 0 && x < W && y >= 0 && y < H) ? g[(size_t)y * W + x] : kOpenOutside;
+    // clamped load: in bounds however the select is compiled
+    const float h = g[(size_t)min(max(y, 0), H - 1) * W + min(max(x, 0), W - 1)];
+    return (x >= 0 && x < W && y >= 0 && y < H) ? h : kOpenOutside;
 }
 
 // Wall voxels of cell (gx, gy) and the side heights their aspect needs.

@@ -48,6 +48,29 @@ def test_trace_matches_oracle(ctx, name):
     np.testing.assert_array_equal(r["barle"], buf)
 
 
+def test_trace_nonfinite_heights_match_oracle(ctx):
+    """Heights of +inf, -inf and NaN, in grid cells (border and interior) and
+    in wall voxels.  The tracer stops rays on a +inf border around its copy
+    of the heightmap; these inputs must still give the reference's lists and
+    shadow bits (viewshed_kernels.cu:31-58: a NaN or +inf start height never
+    hits, a -inf one hits the first finite cell, NaN cells are passed over)."""
+    import dataclasses
+    s = load_scene("dsm64")
+    g = s.grid.copy()
+    W = s.width
+    for x, y, v in [(10, 12, np.inf), (30, 31, -np.inf), (40, 20, np.nan), (0, 0, np.inf), (63, 63, np.nan),
+                    (5, 50, -np.inf), (63, 7, np.inf), (22, 0, np.nan)]:
+        g[y * W + x] = v
+    wz = s.wall_z.copy()
+    wz[[0, 7, 19, 101, 333, 777]] = [np.inf, -np.inf, np.nan, np.inf, -np.inf, np.nan]
+    s2 = dataclasses.replace(s, name="dsm64_nonfinite", grid=g, wall_z=wz)
+    bins, off, ids, sh = oracle_trace(s2)
+    r = ctx.trace(s2, device_arrays(s2))
+    np.testing.assert_array_equal(r["csr_off"], off)
+    np.testing.assert_array_equal(r["csr_ids"], ids)
+    np.testing.assert_array_equal(r["shadow"], sh)
+
+
 def test_dedupe_second_pass_gives_the_same_lists(cuda_lib, scene160):
     """The first-occurrence dedupe first runs with small hash sets and hands
     the rows it gives up on to a second pass with large ones.  With the
