@@ -522,9 +522,10 @@ def run_ours(args, world, rank, local, pg):
     alg = roofline_bytes(scene, (ne.value, nb.value, w.value), args.format, B, args.accumulation, V, entries, staged)
     per_launch_ms = refl_ms / max(1, refl_n)
     achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
-    # slab values delivered to the FMA units per launch (one row of B floats
-    # per entry: through L1, or from shared memory for the tile kernel)
-    gathered = float(entries if V >= 1 else ne.value) * B * 4
+    # slab bytes delivered to the arithmetic per launch: the fp16 union rows
+    # the tensor-core kernel stages into shared memory, else one row of B
+    # floats per entry (through L1, or from shared memory for the tile kernel)
+    gathered = float(staged) * B * 2 if V == 128 else float(entries if V >= 1 else ne.value) * B * 4
     # DRAM bytes per launch come from an ncu capture of this kernel and
     # workload (a profiler run cannot be a timed run); the file is named in
     # the line so that a stale figure can be told from a live one.
@@ -690,6 +691,27 @@ def run_ours(args, world, rank, local, pg):
         extra[f"{FMT_NAMES[ofmt].replace('-', '').lower()}_path"] = {
             "ms_per_step": round(sum(oms) / len(oms), 2), "value": units / (sum(oms) / len(oms) / 1e3),
             "neighbor_format": FMT_NAMES[ofmt]}
+        # The annual-sum form of the same path: Stage 1 as above, then each
+        # voxel's own hours summed once (FP64) and one sparse product with the
+        # sums of its neighbor cells (sum_h sum_g w I = sum_g w sum_h I, the
+        # reference's per-hour reflection being linear in I).  Reported beside
+        # the headline, whose hour-block product is the method the metric names.
+        aopts = dict(opts, reflection=1, time_kernels=0)
+        ctx.run_device(scene, d, out, stream=stream.cuda_stream, **aopts)
+        ams = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.run_device(scene, d, out, stream=stream.cuda_stream, **aopts)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ams.append(e0.elapsed_time(e1))
+        extra["annual_sum_path"] = {
+            "ms_per_step": round(sum(ams) / len(ams), 2), "value": units / (sum(ams) / len(ams) / 1e3),
+            "method": "reflection=annual: Stage 1, then FP64 sums of every voxel's own hours and one sparse "
+                      "product over the weighted lists (k_solar_sum, k_reflect_annual)"}
         ctx.run_device(scene, d, out, stream=stream.cuda_stream, **opts)
         torch.cuda.synchronize(dev)
     if rank == 0 and not args.no_check:
@@ -714,6 +736,13 @@ def run_ours(args, world, rank, local, pg):
             "max_rel": float(rel.max()), "mean_rel": float(rel.mean()), "voxels": int(psmp.size),
             "oracle": "FP64 annual-sum oracle on oracle-built lists and shadow words (the sample's own traces and "
                       "traces of every top cell its lists name); denominator floor 1 Wh/m^2"}
+        if "annual_sum_path" in extra:
+            ctx.run_device(scene, d, out, stream=stream.cuda_stream, **dict(opts, reflection=1, time_kernels=0))
+            torch.cuda.synchronize(dev)
+            ga = out.cpu().numpy().astype(np.float64)
+            rel_a = np.abs(ga[psmp] - orc["annual"]) / np.maximum(np.abs(orc["annual"]), 1.0)
+            extra["annual_sum_path"]["error_vs_fp64_oracle_lists"] = {
+                "max_rel": float(rel_a.max()), "mean_rel": float(rel_a.mean()), "voxels": int(psmp.size)}
         tot, _ = O.annual_fp64(scene, r["shadow"], r["csr_off"], r["csr_ids"])
         rel = np.abs(got - tot) / np.maximum(np.abs(tot), 1.0)
         extra["error_vs_fp64"] = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),

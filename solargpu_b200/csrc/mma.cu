@@ -23,9 +23,11 @@
 //   producers (4 warps)  copy each chunk's 64 union rows of the fp16 slab
 //                        (I[g][256 hours], 512 B a row) with 16-byte cp.async
 //                        straight into the MN-major 128-byte-swizzled layout
-//                        the MMA reads (B operand, N = hours), then fence the
-//                        async proxy and arrive on the stage's full barrier;
-//   builders (3 warps)   zero the stage's W tiles (K-major, 128-byte swizzle,
+//                        the MMA reads (B operand, N = hours) -- 4 slab
+//                        stages, the copies of 3 chunks in flight -- then
+//                        fence the async proxy and arrive on the stage's
+//                        full barrier;
+//   builders (3 warps)   zero one of 2 W stages (K-major, 128-byte swizzle,
 //                        A operand, M = voxels) and scatter the chunk's
 //                        entries, fence, arrive;
 //   MMA (1 thread)       tcgen05.mma kind::f16 M128 N256 K16, 4 per chunk
@@ -54,7 +56,9 @@ namespace {
 constexpr int kGroup = 128;                 // voxels per group = MMA M = TMEM lanes
 constexpr int kHours = 256;                 // hours per block = MMA N
 constexpr int kChunk = 64;                  // union rows per stage = MMA K per stage
-constexpr int kStages = 3;
+constexpr int kBStages = 4;                 // slab-row stages (gathered: latency to hide)
+constexpr int kAStages = 2;                 // weight-tile stages (built from registers)
+constexpr int kCopyLag = kBStages - 2;      // a producer publishes chunk k - kCopyLag after issuing chunk k
 constexpr int kUnionCap = 16384;            // distinct cells of a group the build handles
 constexpr int kHashSlots = 2 * kUnionCap;
 constexpr int kBuildThreads = 1024;
@@ -71,12 +75,13 @@ constexpr int kBuilderWarp0 = 9;            // warps 9-11
 constexpr int kBuilderWarps = 3;
 constexpr int kThreads = 12 * 32;
 
-// shared-memory stage: W hi tile | W lo tile | slab rows
+// shared memory: 2 x (W hi tile | W lo tile), 4 x slab rows, hour table
 constexpr int kTileA = kGroup * kChunk * 2;        // 16 KB, fp16 [128][64], K-major, 128B swizzle
 constexpr int kTileB = kChunk * kHours * 2;        // 32 KB, fp16 [64 rows][256 hours], MN-major, 128B swizzle
-constexpr int kStageBytes = 2 * kTileA + kTileB;   // 64 KB
+constexpr int kAStageBytes = 2 * kTileA;           // 32 KB: hi and lo tiles
+constexpr int kBRegion = kAStages * kAStageBytes;  // slab stages start here
 constexpr int kTableBytes = kHours * (int)sizeof(HourEntry);
-constexpr int kSmemBytes = kStages * kStageBytes + kTableBytes + 1024;   // + 1024-byte alignment slack
+constexpr int kSmemBytes = kBRegion + kBStages * kTileB + kTableBytes + 1024;   // + 1024-byte alignment slack
 
 // Instruction descriptor, kind::f16: f32 accumulator, fp16 A and B, A
 // K-major, B MN-major, N = 256, M = 128.
@@ -370,7 +375,9 @@ struct MmaTiles {
 struct Cursor {
     int q, c, u, step, NG;
     long long ub;   // first union cell of group q
-    __device__ Cursor(const MmaTiles& mt, int first, int stride) : q(first), c(0), u(0), step(stride), NG(mt.NG), ub(0)
+    long long cb;   // first chunk of group q
+    __device__ Cursor(const MmaTiles& mt, int first, int stride)
+        : q(first), c(0), u(0), step(stride), NG(mt.NG), ub(0), cb(0)
     {
         settle(mt);
     }
@@ -381,7 +388,10 @@ struct Cursor {
             u = __ldg(mt.unions + q);
             if (c * kChunk < u) break;
         }
-        if (q < NG) ub = __ldg(mt.woff + (long long)q * kGroup);
+        if (q < NG) {
+            ub = __ldg(mt.woff + (long long)q * kGroup);
+            cb = __ldg(mt.cbase + q);
+        }
     }
     __device__ void advance(const MmaTiles& mt)
     {
@@ -407,25 +417,28 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
               Accum acc, int* __restrict__ err)
 {
     extern __shared__ __align__(1024) unsigned char dsm[];
-    __shared__ __align__(8) unsigned long long full[kStages], aready[kStages], empty[kStages], dfull[2], dempty[2],
-        drain;
+    __shared__ __align__(8) unsigned long long full[kBStages], emptyB[kBStages], aready[kAStages], emptyA[kAStages],
+        dfull[2], dempty[2], drain;
     __shared__ unsigned s_tmem;
     __shared__ volatile int s_fail;
     __shared__ volatile int s_bok;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned base = (su32(dsm) + 1023u) & ~1023u;               // stages, 1024-byte aligned
     unsigned char* gbase = dsm + (base - su32(dsm));
-    HourEntry* tab = reinterpret_cast<HourEntry*>(gbase + kStages * kStageBytes);
+    HourEntry* tab = reinterpret_cast<HourEntry*>(gbase + kBRegion + kBStages * kTileB);
 
     if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&s_tmem)), "r"(512));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
+        for (int s = 0; s < kBStages; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&full[s])), "r"(kProducerWarps));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&emptyB[s])), "r"(1));
+        }
+        for (int s = 0; s < kAStages; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&aready[s])), "r"(1));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&empty[s])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&emptyA[s])), "r"(1));
         }
         for (int b = 0; b < 2; ++b) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(&dfull[b])), "r"(1));
@@ -445,22 +458,20 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
 
     if (warp < kProducerWarps) {
         // ---- producers: 16 rows a warp, one 16-byte piece a lane per row; the
-        // cell ids of the next chunk are loaded while this one is issued
+        // cell ids of the next chunk load while its stage is still in use
         long long k = 0;
         const int r0 = warp * 16;
         Cursor cur(mt, blockIdx.x, gridDim.x);
         int my = cur.valid() ? cur.row_cell(mt, r0 + lane, lane < 16) : 0;
         while (cur.valid() && ok) {
-            const int s = (int)(k % kStages);
-            const bool w_ok = k < kStages || bar_wait(su32(&empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_fail);
+            const int s = (int)(k % kBStages);
+            const bool w_ok = k < kBStages || bar_wait(su32(&emptyB[s]), (unsigned)(((k / kBStages) - 1) & 1), &s_fail);
             if (!__all_sync(0xFFFFFFFFu, w_ok)) {   // the warp decides as one
                 ok = false;
                 break;
             }
             const int cur_cell = my;
-            cur.advance(mt);
-            my = cur.valid() ? cur.row_cell(mt, r0 + lane, lane < 16) : 0;
-            const unsigned bst = base + (unsigned)(s * kStageBytes) + 2 * kTileA;
+            const unsigned bst = base + (unsigned)(kBRegion + s * kTileB);
             const int na = lane >> 3, cc = lane & 7;
 #pragma unroll 4
             for (int i = 0; i < 16; ++i) {
@@ -472,19 +483,26 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
                 asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
-            if (k >= 1) {
-                // the previous chunk's copies have landed: publish them to the tensor cores
-                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            if (k >= kCopyLag) {
+                // chunk k - 2's copies have landed (the last 2 groups may be
+                // pending): publish them to the tensor cores
+                static_assert(kCopyLag == 2, "wait_group count below");
+                asm volatile("cp.async.wait_group 2;" ::: "memory");
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
-                if (lane == 0) bar_arrive(su32(&full[(k - 1) % kStages]));
+                if (lane == 0) bar_arrive(su32(&full[(k - kCopyLag) % kBStages]));
             }
+            // the next chunk's cell ids (a new group first reads its union
+            // size and base: those loads stay off the copy and arrive path)
+            cur.advance(mt);
+            my = cur.valid() ? cur.row_cell(mt, r0 + lane, lane < 16) : 0;
             ++k;
         }
         asm volatile("cp.async.wait_group 0;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
-        if (k >= 1 && lane == 0) bar_arrive(su32(&full[(k - 1) % kStages]));
+        if (lane == 0)
+            for (long long j = k >= kCopyLag ? k - kCopyLag : 0; j < k; ++j) bar_arrive(su32(&full[j % kBStages]));
         if (!ok) {
             if (lane == 0) atomicOr(err, kErrWaitTimeout);
             s_fail = 1;
@@ -504,22 +522,24 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
                 const int u = mt.unions[q];
                 const unsigned d = tmem + (unsigned)(b * kHours);
                 for (int c = 0; c * kChunk < u; ++c, ++k) {
-                    const int s = (int)(k % kStages);
-                    const unsigned ph = (unsigned)((k / kStages) & 1);
-                    if (!bar_wait(su32(&full[s]), ph, &s_fail) || !bar_wait(su32(&aready[s]), ph, &s_fail)) {
+                    const int s = (int)(k % kBStages), t = (int)(k % kAStages);
+                    if (!bar_wait(su32(&full[s]), (unsigned)((k / kBStages) & 1), &s_fail) ||
+                        !bar_wait(su32(&aready[t]), (unsigned)((k / kAStages) & 1), &s_fail)) {
                         ok = false;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const unsigned sa = base + (unsigned)(s * kStageBytes);
-                    const unsigned sb = sa + 2 * kTileA;
+                    const unsigned sa = base + (unsigned)(t * kAStageBytes);
+                    const unsigned sb = base + (unsigned)(kBRegion + s * kTileB);
                     const int ks = (min(kChunk, u - c * kChunk) + 15) >> 4;
                     for (int j = 0; j < ks; ++j) {
                         const unsigned long long db = desc_mn_sw128(sb + 2048u * j);
                         mma_f16(d, desc_k_sw128(sa + 32u * j), db, (c > 0 || j > 0) ? 1u : 0u);
                         mma_f16(d, desc_k_sw128(sa + kTileA + 32u * j), db, 1u);
                     }
-                    mma_commit(su32(&empty[s]));   // the stage is free once these MMAs have read it
+                    // both stages are free once these MMAs have read them
+                    mma_commit(su32(&emptyB[s]));
+                    mma_commit(su32(&emptyA[t]));
                 }
                 if (!ok) break;
                 mma_commit(su32(&dfull[b]));       // the group's accumulator is complete
@@ -543,7 +563,7 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         auto prefetch = [&]() {
             pe0 = pe1 = 0;
             if (cur.valid()) {
-                const long long ci = __ldg(mt.cbase + cur.q) + cur.c;
+                const long long ci = cur.cb + cur.c;
                 pe0 = __ldg(mt.coff + ci);
                 pe1 = __ldg(mt.coff + ci + 1);
             }
@@ -556,15 +576,15 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         prefetch();
         long long k = 0;
         while (cur.valid() && ok) {
-            const int s = (int)(k % kStages);
+            const int s = (int)(k % kAStages);
             // one thread waits for the stage; every builder takes its decision
             if (bt == 0)
-                s_bok = (k < kStages || bar_wait(su32(&empty[s]), (unsigned)(((k / kStages) - 1) & 1), &s_fail))
+                s_bok = (k < kAStages || bar_wait(su32(&emptyA[s]), (unsigned)(((k / kAStages) - 1) & 1), &s_fail))
                             ? 1 : 0;
             asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
             ok = s_bok != 0;
             if (!ok) break;
-            unsigned char* sa = gbase + (size_t)s * kStageBytes;
+            unsigned char* sa = gbase + (size_t)s * kAStageBytes;
             uint4* z = reinterpret_cast<uint4*>(sa);
             for (int i = bt; i < 2 * kTileA / 16; i += kBuilders) z[i] = make_uint4(0u, 0u, 0u, 0u);
             asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
@@ -580,11 +600,13 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
                 *reinterpret_cast<unsigned short*>(sa + en.x) = (unsigned short)(en.y & 0xFFFFu);
                 *reinterpret_cast<unsigned short*>(sa + kTileA + en.x) = (unsigned short)(en.y >> 16);
             }
-            cur.advance(mt);
-            prefetch();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("bar.sync 1, %0;" ::"r"(kBuilders) : "memory");
             if (bt == 0) bar_arrive(su32(&aready[s]));
+            // the next chunk's entries load while the builders wait for its stage
+            // (after the arrive: their latency stays off the MMA's path)
+            cur.advance(mt);
+            prefetch();
             ++k;
         }
         if (!ok) {
