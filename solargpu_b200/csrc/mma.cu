@@ -27,7 +27,7 @@
 //                        stages, the copies of 3 chunks in flight -- then
 //                        fence the async proxy and arrive on the stage's
 //                        full barrier;
-//   builders (3 warps)   zero one of 2 W stages (K-major, 128-byte swizzle,
+//   builders (3 warps)   zero one of 3 W stages (K-major, 128-byte swizzle,
 //                        A operand, M = voxels) and scatter the chunk's
 //                        entries, fence, arrive;
 //   MMA (1 thread)       tcgen05.mma kind::f16 M128 N256 K16, 4 per chunk
@@ -47,6 +47,10 @@
 #include "solar_math.cuh"
 
 #include <atomic>
+#include <functional>
+#include <queue>
+#include <utility>
+#include <vector>
 
 #include <cuda_fp16.h>
 
@@ -57,7 +61,7 @@ constexpr int kGroup = 128;                 // voxels per group = MMA M = TMEM l
 constexpr int kHours = 256;                 // hours per block = MMA N
 constexpr int kChunk = 64;                  // union rows per stage = MMA K per stage
 constexpr int kBStages = 4;                 // slab-row stages (gathered: latency to hide)
-constexpr int kAStages = 2;                 // weight-tile stages (built from registers)
+constexpr int kAStages = 3;                 // weight-tile stages (built from registers)
 constexpr int kCopyLag = kBStages - 2;      // a producer publishes chunk k - kCopyLag after issuing chunk k
 constexpr int kUnionCap = 16384;            // distinct cells of a group the build handles
 constexpr int kHashSlots = 2 * kUnionCap;
@@ -75,13 +79,14 @@ constexpr int kBuilderWarp0 = 9;            // warps 9-11
 constexpr int kBuilderWarps = 3;
 constexpr int kThreads = 12 * 32;
 
-// shared memory: 2 x (W hi tile | W lo tile), 4 x slab rows, hour table
+// shared memory: 3 x (W hi tile | W lo tile), 4 x slab rows (the hour table
+// is read through L1: every epilogue lane reads the same entry)
 constexpr int kTileA = kGroup * kChunk * 2;        // 16 KB, fp16 [128][64], K-major, 128B swizzle
 constexpr int kTileB = kChunk * kHours * 2;        // 32 KB, fp16 [64 rows][256 hours], MN-major, 128B swizzle
 constexpr int kAStageBytes = 2 * kTileA;           // 32 KB: hi and lo tiles
 constexpr int kBRegion = kAStages * kAStageBytes;  // slab stages start here
-constexpr int kTableBytes = kHours * (int)sizeof(HourEntry);
-constexpr int kSmemBytes = kBRegion + kBStages * kTileB + kTableBytes + 1024;   // + 1024-byte alignment slack
+constexpr int kSmemBytes = kBRegion + kBStages * kTileB + 1024;   // 225 KB + 1024-byte alignment slack
+static_assert(kSmemBytes <= 227 * 1024 - 512, "dynamic + static shared memory of one CTA");
 
 // Instruction descriptor, kind::f16: f32 accumulator, fp16 A and B, A
 // K-major, B MN-major, N = 256, M = 128.
@@ -367,28 +372,31 @@ struct MmaTiles {
     const long long* coff;     // [C + 1] first entry of each chunk
     const uint2* ent;          // entries: x = byte offset in the W tile, y = half2 (hi, lo)
     const float* scale;        // [N] 2^e per visiting position
+    const int* sched;          // [gridDim.x + 1] offsets, then the groups of each CTA
 };
 
-// Walks the (group, chunk) sequence of one CTA: groups blockIdx.x,
-// blockIdx.x + gridDim.x, ..., chunks of 64 union rows inside each group
-// (groups with an empty union have none) -- the order every role follows.
+// Walks the (group, chunk) sequence of one CTA: the CTA's groups in its
+// schedule, chunks of 64 union rows inside each group (groups with an empty
+// union have none) -- the order every role follows.
 struct Cursor {
-    int q, c, u, step, NG;
+    int i, iend, q, c, u;
     long long ub;   // first union cell of group q
     long long cb;   // first chunk of group q
-    __device__ Cursor(const MmaTiles& mt, int first, int stride)
-        : q(first), c(0), u(0), step(stride), NG(mt.NG), ub(0), cb(0)
+    __device__ Cursor(const MmaTiles& mt, int cta)
+        : i(__ldg(mt.sched + cta)), iend(__ldg(mt.sched + cta + 1)), q(0), c(0), u(0), ub(0), cb(0)
     {
         settle(mt);
     }
-    __device__ bool valid() const { return q < NG; }
+    __device__ bool valid() const { return i < iend; }
     __device__ void settle(const MmaTiles& mt)
     {
-        for (; q < NG; q += step, c = 0) {
+        const int* list = mt.sched + gridDim.x + 1;
+        for (; i < iend; ++i, c = 0) {
+            q = __ldg(list + i);
             u = __ldg(mt.unions + q);
             if (c * kChunk < u) break;
         }
-        if (q < NG) {
+        if (i < iend) {
             ub = __ldg(mt.woff + (long long)q * kGroup);
             cb = __ldg(mt.cbase + q);
         }
@@ -397,7 +405,7 @@ struct Cursor {
     {
         ++c;
         if (c * kChunk >= u) {
-            q += step;
+            ++i;
             c = 0;
             settle(mt);
         }
@@ -425,7 +433,7 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned base = (su32(dsm) + 1023u) & ~1023u;               // stages, 1024-byte aligned
     unsigned char* gbase = dsm + (base - su32(dsm));
-    HourEntry* tab = reinterpret_cast<HourEntry*>(gbase + kBRegion + kBStages * kTileB);
+    const HourEntry* tab = table + j0;
 
     if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&s_tmem)), "r"(512));
@@ -448,8 +456,6 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
     }
-    // the block's hour table
-    for (int i = threadIdx.x; i < kHours; i += blockDim.x) tab[i] = table[j0 + i];
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -461,7 +467,7 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         // cell ids of the next chunk load while its stage is still in use
         long long k = 0;
         const int r0 = warp * 16;
-        Cursor cur(mt, blockIdx.x, gridDim.x);
+        Cursor cur(mt, blockIdx.x);
         int my = cur.valid() ? cur.row_cell(mt, r0 + lane, lane < 16) : 0;
         while (cur.valid() && ok) {
             const int s = (int)(k % kBStages);
@@ -512,7 +518,10 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         if (lane == 0) {
             long long k = 0;
             int gi = 0;
-            for (int q = blockIdx.x; q < mt.NG && ok; q += gridDim.x, ++gi) {
+            const int* list = mt.sched + gridDim.x + 1;
+            const int i1 = __ldg(mt.sched + blockIdx.x + 1);
+            for (int i = __ldg(mt.sched + blockIdx.x); i < i1 && ok; ++i, ++gi) {
+                const int q = __ldg(list + i);
                 const int b = gi & 1;
                 if (gi >= 2 && !bar_wait(su32(&dempty[b]), (unsigned)(((gi >> 1) - 1) & 1), &s_fail)) {
                     ok = false;
@@ -557,7 +566,7 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         const int bt = threadIdx.x - kBuilderWarp0 * 32;
         constexpr int kBuilders = kBuilderWarps * 32;
         constexpr int kPref = 12;   // entries a thread holds ahead; more are loaded at scatter time
-        Cursor cur(mt, blockIdx.x, gridDim.x);
+        Cursor cur(mt, blockIdx.x);
         uint2 pre[kPref];
         long long pe0 = 0, pe1 = 0;
         auto prefetch = [&]() {
@@ -618,7 +627,10 @@ k_reflect_mma(const __half* __restrict__ slab, MmaTiles mt, const float4* __rest
         const int t = threadIdx.x - kEpilogueWarp0 * 32;
         const unsigned lane_base = (unsigned)((warp & 3) * 32) << 16;
         int gi = 0;
-        for (int q = blockIdx.x; q < mt.NG && ok; q += gridDim.x, ++gi) {
+        const int* list = mt.sched + gridDim.x + 1;
+        const int i1 = __ldg(mt.sched + blockIdx.x + 1);
+        for (int i = __ldg(mt.sched + blockIdx.x); i < i1 && ok; ++i, ++gi) {
+            const int q = __ldg(list + i);
             const int b = gi & 1;
             const bool w_ok = bar_wait(su32(&dfull[b]), (unsigned)((gi >> 1) & 1), &s_fail, 2 * kWaitNs);
             if (!__all_sync(0xFFFFFFFFu, w_ok)) {   // tcgen05.ld below needs the whole warp
@@ -711,6 +723,38 @@ cudaError_t allow_smem(K kernel, size_t bytes, std::atomic<bool> (&done)[kMaxDev
 
 int mma_group_count(int N) { return (N + kGroup - 1) / kGroup; }
 
+int mma_grid(int N)
+{
+    const int NG = mma_group_count(N);
+    return NG < mma_sms() ? NG : mma_sms();
+}
+
+void mma_schedule(int N, const long long* cbase, int* sched)
+{
+    const int NG = mma_group_count(N);
+    const int P = mma_grid(N);
+    if (NG <= 0 || P <= 0) return;
+    // a group costs its chunks plus about one chunk of switching (the epilogue
+    // of its accumulator, the first copies of the next group)
+    constexpr long long kGroupCost = 1;
+    std::vector<int> owner(NG), count(P, 0);
+    std::priority_queue<std::pair<long long, int>, std::vector<std::pair<long long, int>>,
+                        std::greater<std::pair<long long, int>>> load;
+    for (int b = 0; b < P; ++b) load.push({0, b});
+    for (int q = 0; q < NG; ++q) {
+        const auto top = load.top();
+        load.pop();
+        owner[q] = top.second;
+        ++count[top.second];
+        load.push({top.first + (cbase[q + 1] - cbase[q]) + kGroupCost, top.second});
+    }
+    sched[0] = 0;
+    for (int b = 0; b < P; ++b) sched[b + 1] = sched[b] + count[b];
+    std::vector<int> at(sched, sched + P);
+    int* list = sched + P + 1;
+    for (int q = 0; q < NG; ++q) list[at[owner[q]]++] = q;   // increasing within each CTA
+}
+
 cudaError_t launch_mma_union(int N, const long long* woff, int* cells, unsigned short* slots, int* unions, int* nch,
                              int* over, cudaStream_t st)
 {
@@ -756,9 +800,10 @@ cudaError_t launch_reflect_mma(const void* slab16, const MmaLists& ml, const Dev
     static std::atomic<bool> attr[kMaxDevices];
     cudaError_t e = allow_smem(k_reflect_mma, (size_t)kSmemBytes, attr);
     if (e != cudaSuccess) return e;
+    if (!ml.sched) return cudaErrorInvalidValue;
     MmaTiles mt{ml.N, NG, ml.order, ml.woff, ml.cells, ml.unions, ml.cbase, ml.coff,
-                reinterpret_cast<const uint2*>(ml.ent), ml.scale};
-    const int grid = NG < mma_sms() ? NG : mma_sms();
+                reinterpret_cast<const uint2*>(ml.ent), ml.scale, ml.sched};
+    const int grid = mma_grid(ml.N);
     k_reflect_mma<<<grid, kThreads, kSmemBytes, st>>>(static_cast<const __half*>(slab16), mt, g.geo_n, shadow,
                                                        words32, table, j0, acc, err);
     return cudaGetLastError();

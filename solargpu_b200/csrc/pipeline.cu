@@ -111,7 +111,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp, gpad;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp, gpad, mma_sched;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -139,7 +139,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 79;
+static constexpr int kNumBufs = 80;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -721,6 +721,17 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                     ml.coff = as<long long>(c->mma_coff);
                     ml.ent = c->mma_ent.p;
                     ml.scale = as<float>(c->mma_scale);
+                    // balanced group order over the CTAs of the hour-block kernel
+                    std::vector<long long> cb((size_t)NG + 1);
+                    CK(cudaMemcpyAsync(cb.data(), c->mma_cbase.p, sizeof(long long) * ((size_t)NG + 1),
+                                       cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    std::vector<int> sched((size_t)mma_grid(N) + 1 + NG);
+                    mma_schedule(N, cb.data(), sched.data());
+                    RK(ensure(c, c->mma_sched, sizeof(int) * sched.size()));
+                    CK(cudaMemcpyAsync(c->mma_sched.p, sched.data(), sizeof(int) * sched.size(), cudaMemcpyHostToDevice,
+                                       st));
+                    ml.sched = as<int>(c->mma_sched);
                 }
             }
             if (mma) {
@@ -1166,7 +1177,7 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
                                 &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
-                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp, &c->gpad};
+                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp, &c->gpad, &c->mma_sched};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

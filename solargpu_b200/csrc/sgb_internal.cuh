@@ -221,11 +221,20 @@ struct MmaLists {
     const long long* coff;     // [chunks + 1] first entry of each chunk
     const void* ent;           // [entries] 8 bytes: W-tile byte offset, fp16 hi, fp16 lo
     const float* scale;        // [N] per visiting position: 2^e undoing the weight scaling
+    const int* sched;          // [mma_grid + 1 + groups]: per-CTA offsets, then the groups of each CTA
 };
 constexpr int kMmaGroup = 128;
 constexpr int kMmaHours = 256;
 constexpr int kMmaChunk = 64;
 int mma_group_count(int N);
+// CTAs of the hour-block kernel for N voxels (the schedule is made for them).
+int mma_grid(int N);
+// Balanced static schedule of the groups over mma_grid(N) CTAs: in visiting
+// order, each group goes to the CTA with the least work so far (its chunks
+// plus a per-group cost), as a dynamic scheduler would hand them out, so
+// neighbouring groups still run at the same time.  cbase [groups + 1] on the
+// host; sched receives mma_grid + 1 offsets followed by the groups.
+void mma_schedule(int N, const long long* cbase, int* sched);
 // Union of each group (cells rewritten in place, slots per entry, union size
 // and chunk count per group); *over counts groups above the union cap.
 cudaError_t launch_mma_union(int N, const long long* woff, int* cells, unsigned short* slots, int* unions, int* nch,
