@@ -47,6 +47,7 @@
 #include "solar_math.cuh"
 
 #include <atomic>
+#include <cstdlib>
 #include <functional>
 #include <queue>
 #include <utility>
@@ -65,6 +66,7 @@ constexpr int kAStages = 3;                 // weight-tile stages (built from re
 constexpr int kCopyLag = kBStages - 2;      // a producer publishes chunk k - kCopyLag after issuing chunk k
 constexpr int kUnionCap = 16384;            // distinct cells of a group the build handles
 constexpr int kHashSlots = 2 * kUnionCap;
+constexpr int kSmallCap = 8192;             // first pass: unions up to this many cells
 constexpr int kBuildThreads = 1024;
 constexpr int kLayoutThreads = 512;
 constexpr int kMaxChunks = kUnionCap / kChunk;
@@ -113,48 +115,42 @@ __device__ __forceinline__ void block_sort_desc(uint32_t* keys, int n2)
     }
 }
 
-// One CTA per group of 128 positions.  cells[e] (0-based cell of weighted
-// entry e) are replaced, from woff[p0] on, by the group's union (descending);
-// slots[e] = index of the entry's cell in it.  A union above kUnionCap cells
-// leaves the group untouched and counts it in *over.
-__global__ void __launch_bounds__(kBuildThreads)
-k_mma_union(int N, const long long* __restrict__ woff, int* __restrict__ cells, unsigned short* __restrict__ slots,
-            int* __restrict__ unions, int* __restrict__ nch, int* __restrict__ over)
+// The union of group q, in one CTA: cells[e] (0-based cell of weighted entry
+// e) are replaced, from woff[p0] on, by the group's union (descending);
+// slots[e] = index of the entry's cell in it.  Returns false, writing
+// nothing, when the union has more than CAP cells.
+template <int CAP>
+__device__ bool union_group(int q, int N, const long long* __restrict__ woff, int* __restrict__ cells,
+                            unsigned short* __restrict__ slots, int* __restrict__ unions, int* __restrict__ nch,
+                            uint32_t* sm, int* s_count)
 {
-    extern __shared__ __align__(16) uint32_t sm[];
-    uint32_t* table = sm;                 // [kHashSlots], key = cell + 1, 0 = empty
-    uint32_t* uni = sm + kHashSlots;      // [kUnionCap]
-    __shared__ int s_count;
-    const int q = blockIdx.x;
+    constexpr int kSlots = 2 * CAP;
+    constexpr int kBits = CAP == 16384 ? 15 : CAP == 8192 ? 14 : 0;
+    static_assert(kBits > 0, "union cap of 8192 or 16384 cells");
+    uint32_t* table = sm;                 // [kSlots], key = cell + 1, 0 = empty
+    uint32_t* uni = sm + kSlots;          // [CAP]
     const int p0 = q * kGroup, p1 = min(N, p0 + kGroup);
     const long long e0 = woff[p0], e1 = woff[p1];
-    for (int i = threadIdx.x; i < kHashSlots; i += blockDim.x) table[i] = 0u;
-    if (threadIdx.x == 0) s_count = 0;
+    for (int i = threadIdx.x; i < kSlots; i += blockDim.x) table[i] = 0u;
+    if (threadIdx.x == 0) *s_count = 0;
     __syncthreads();
     for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const uint32_t key = (uint32_t)cells[e] + 1u;
-        uint32_t h = (key * 2654435761u) >> 17;   // 15 bits
-        for (int probe = 0; probe < kHashSlots; ++probe) {
+        uint32_t h = (key * 2654435761u) >> (32 - kBits);
+        for (int probe = 0; probe < kSlots; ++probe) {
             const uint32_t prev = atomicCAS(&table[h], 0u, key);
             if (prev == 0u) {
-                const int at = atomicAdd(&s_count, 1);
-                if (at < kUnionCap) uni[at] = key;
+                const int at = atomicAdd(s_count, 1);
+                if (at < CAP) uni[at] = key;
                 break;
             }
             if (prev == key) break;
-            h = (h + 1u) & (kHashSlots - 1);
+            h = (h + 1u) & (kSlots - 1);
         }
     }
     __syncthreads();
-    const int u = s_count;
-    if (u > kUnionCap) {
-        if (threadIdx.x == 0) {
-            atomicAdd(over, 1);
-            unions[q] = 0;
-            nch[q] = 0;
-        }
-        return;
-    }
+    const int u = *s_count;
+    if (u > CAP) return false;   // uniform: every thread read the same count
     int u2 = 64;
     while (u2 < u) u2 <<= 1;
     for (int i = u + threadIdx.x; i < u2; i += blockDim.x) uni[i] = 0u;
@@ -177,6 +173,44 @@ k_mma_union(int N, const long long* __restrict__ woff, int* __restrict__ cells, 
     if (threadIdx.x == 0) {
         unions[q] = u;
         nch[q] = (u + kChunk - 1) / kChunk;
+    }
+    return true;
+}
+
+// First pass, one CTA per group with room for kSmallCap cells (96 KB of
+// shared memory: two CTAs a SM); a group with a larger union is listed in
+// retry[1 ..] (count in retry[0]) and left untouched.
+__global__ void __launch_bounds__(kBuildThreads)
+k_mma_union_small(int N, const long long* __restrict__ woff, int* __restrict__ cells,
+                  unsigned short* __restrict__ slots, int* __restrict__ unions, int* __restrict__ nch,
+                  int* __restrict__ retry, int hand_on_all)
+{
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ int s_count;
+    const int q = blockIdx.x;
+    if ((hand_on_all || !union_group<kSmallCap>(q, N, woff, cells, slots, unions, nch, sm, &s_count)) &&
+        threadIdx.x == 0)
+        retry[1 + atomicAdd(retry, 1)] = q;
+}
+
+// Second pass over the listed groups with room for kUnionCap cells; a union
+// above that leaves the group untouched and counts it in *over.
+__global__ void __launch_bounds__(kBuildThreads)
+k_mma_union_large(int N, const long long* __restrict__ woff, int* __restrict__ cells,
+                  unsigned short* __restrict__ slots, int* __restrict__ unions, int* __restrict__ nch,
+                  const int* __restrict__ retry, int* __restrict__ over)
+{
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ int s_count;
+    const int n = retry[0];
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int q = retry[1 + i];
+        if (!union_group<kUnionCap>(q, N, woff, cells, slots, unions, nch, sm, &s_count) && threadIdx.x == 0) {
+            atomicAdd(over, 1);
+            unions[q] = 0;
+            nch[q] = 0;
+        }
+        __syncthreads();
     }
 }
 
@@ -756,15 +790,25 @@ void mma_schedule(int N, const long long* cbase, int* sched)
 }
 
 cudaError_t launch_mma_union(int N, const long long* woff, int* cells, unsigned short* slots, int* unions, int* nch,
-                             int* over, cudaStream_t st)
+                             int* over, int* retry, cudaStream_t st)
 {
     const int NG = mma_group_count(N);
     if (NG <= 0) return cudaSuccess;
-    const size_t smem = sizeof(uint32_t) * (size_t)(kHashSlots + kUnionCap);
-    static std::atomic<bool> attr[kMaxDevices];
-    cudaError_t e = allow_smem(k_mma_union, smem, attr);
+    cudaError_t e = cudaMemsetAsync(retry, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    k_mma_union<<<NG, kBuildThreads, smem, st>>>(N, woff, cells, slots, unions, nch, over);
+    const size_t small = sizeof(uint32_t) * (size_t)(3 * kSmallCap);
+    const size_t large = sizeof(uint32_t) * (size_t)(kHashSlots + kUnionCap);
+    static std::atomic<bool> attr_s[kMaxDevices], attr_l[kMaxDevices];
+    if ((e = allow_smem(k_mma_union_small, small, attr_s)) != cudaSuccess) return e;
+    if ((e = allow_smem(k_mma_union_large, large, attr_l)) != cudaSuccess) return e;
+    // SGB_UNION_SECOND_PASS=1 hands every group to the second pass (tests use
+    // it to check that pass; the unions are the same either way)
+    const char* env = std::getenv("SGB_UNION_SECOND_PASS");
+    const int all = (env && env[0] == '1') ? 1 : 0;
+    k_mma_union_small<<<NG, kBuildThreads, small, st>>>(N, woff, cells, slots, unions, nch, retry, all);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // the groups the first pass listed (usually few; the grid exits at once when none)
+    k_mma_union_large<<<mma_sms(), kBuildThreads, large, st>>>(N, woff, cells, slots, unions, nch, retry, over);
     return cudaGetLastError();
 }
 

@@ -111,7 +111,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp, gpad, mma_sched;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp, gpad, mma_sched, mma_retry;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -139,7 +139,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 80;
+static constexpr int kNumBufs = 81;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -662,12 +662,13 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
                 RK(ensure(c, c->mma_nch, sizeof(int) * (size_t)NG));
                 RK(ensure(c, c->mma_cbase, sizeof(long long) * ((size_t)NG + 1)));
                 RK(ensure(c, c->mma_over, sizeof(long long)));
+                RK(ensure(c, c->mma_retry, sizeof(int) * ((size_t)NG + 1)));
                 {
                     KScope k(c, SOLAR_GPU_KT_GROUP);
                     CK(cudaMemsetAsync(c->mma_over.p, 0, sizeof(long long), st));
                     CK(launch_mma_union(N, as<long long>(c->w_off), as<int>(c->w_cell),
                                         as<unsigned short>(c->tile_slot), as<int>(c->mma_union), as<int>(c->mma_nch),
-                                        as<int>(c->mma_over), st));
+                                        as<int>(c->mma_over), as<int>(c->mma_retry), st));
                     CK(launch_scan_counts(as<int>(c->mma_nch), NG, 0, as<long long>(c->mma_cbase),
                                           as<long long>(c->w_tmp), nullptr, st));
                 }
@@ -1177,7 +1178,7 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
                                 &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
-                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp, &c->gpad, &c->mma_sched};
+                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp, &c->gpad, &c->mma_sched, &c->mma_retry};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

@@ -237,8 +237,9 @@ int mma_grid(int N);
 void mma_schedule(int N, const long long* cbase, int* sched);
 // Union of each group (cells rewritten in place, slots per entry, union size
 // and chunk count per group); *over counts groups above the union cap.
+// retry: groups + 1 ints of scratch (groups the small first pass hands on).
 cudaError_t launch_mma_union(int N, const long long* woff, int* cells, unsigned short* slots, int* unions, int* nch,
-                             int* over, cudaStream_t st);
+                             int* over, int* retry, cudaStream_t st);
 // pass 0: entries per chunk (ccnt at cbase) and the per-position scale;
 // pass 1: the entries at coff (the scan of ccnt).
 cudaError_t launch_mma_layout(int pass, int N, const long long* woff, const unsigned short* slots, const float* wts,

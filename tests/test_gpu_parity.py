@@ -95,6 +95,39 @@ def test_dedupe_second_pass_gives_the_same_lists(cuda_lib, scene160):
     assert p.returncode == 0 and "same lists" in p.stdout, p.stdout + p.stderr
 
 
+def test_union_second_pass_gives_the_same_result(cuda_lib, scene160, tmp_path):
+    """The group unions of the tensor-core kernel are built by a first pass
+    with room for 8192 cells a group and a second pass, with room for 16384,
+    for the groups the first hands on.  With every group handed on
+    (SGB_UNION_SECOND_PASS=1) the irradiance must be bit-identical to the
+    default run.  Runs in a child process so the setting stays out of the
+    other tests."""
+    import os
+    import subprocess
+    import sys
+    import torch
+    from solargpu_b200 import api
+    from conftest import ROOT
+    out = torch.zeros(scene160.num_total, dtype=torch.float32, device="cuda:0")
+    with api.Context(0) as c:
+        c.run_device(scene160, device_arrays(scene160), out, neighbor_format=0, hour_block=256, group_size=128)
+    want = out.cpu().numpy()
+    code = (
+        "import sys, numpy as np, torch; sys.path.insert(0, 'tests'); sys.path.insert(0, '.');"
+        "from conftest import load_scene, device_arrays;"
+        "from solargpu_b200 import api;"
+        "s = load_scene('dsm160'); out = torch.zeros(s.num_total, dtype=torch.float32, device='cuda:0');"
+        "c = api.Context(0); c.run_device(s, device_arrays(s), out, neighbor_format=0, hour_block=256, group_size=128);"
+        "np.save(sys.argv[1], out.cpu().numpy()); print('ran')")
+    path = str(tmp_path / "second_pass.npy")
+    env = dict(os.environ, SGB_UNION_SECOND_PASS="1")
+    p = subprocess.run([sys.executable, "-c", code, path], cwd=ROOT, env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0 and "ran" in p.stdout, p.stdout + p.stderr
+    got = np.load(path)
+    assert np.array_equal(got.view(np.int32), want.view(np.int32))
+
+
 def test_trace_chunked_equals_single(ctx, scene160):
     dev = device_arrays(scene160)
     a = ctx.trace(scene160, dev)
