@@ -12,8 +12,8 @@
 // run optimiser is the reference's sequential fixpoint and runs on one lane
 // over the (short) run list; payload bytes are written lane-parallel.
 // Two passes: k_barle_size computes each stream's byte count (and leaves the
-// sorted list in place), a scan turns counts into offsets, k_barle_write
-// packs the bytes.
+// sorted list and, room permitting, its optimised runs in the row), a scan
+// turns counts into offsets, k_barle_write packs the bytes.
 #include "sgb_internal.cuh"
 
 namespace sgb {
@@ -165,6 +165,14 @@ k_barle_size(int chunk_count, int D, int* __restrict__ raw, const int* __restric
     load_sorted(row, k, ids, lane, true);
     for (int i = lane; i < k; i += 32) row[i] = (int)ids[i];   // keep the sorted list for the write pass
     const int nr = build_runs(ids, k, runs, lane);
+    // and, where the row has room after the list, its optimised runs (the
+    // write pass then skips build_runs): row[k] = run count, runs after it
+    if (k < D) {
+        const bool fits = k + 1 + nr <= D;
+        if (lane == 0) row[k] = fits ? nr : -1;
+        if (fits)
+            for (int r = lane; r < nr; r += 32) row[k + 1 + r] = (int)runs[r];
+    }
     int pieces = 0, payload = 0;
     for (int r = lane; r < nr; r += 32) {
         const int w = run_w(runs[r]), len = run_len(runs[r]);
@@ -197,7 +205,14 @@ k_barle_write(int chunk_count, int D, const int* __restrict__ raw, const int* __
     if (k <= 0 || k > D || k > RUNS) return;
     const int* row = raw + (size_t)(inv ? inv[lv] : lv) * D;
     load_sorted(row, k, ids, lane, false);   // already sorted by k_barle_size
-    int nr = build_runs(ids, k, runs, lane);
+    // the runs k_barle_size left after the list, else built again
+    int nr = k < D ? row[k] : -1;
+    if (nr >= 0 && k + 1 + nr <= D) {
+        for (int r = lane; r < nr; r += 32) runs[r] = (uint32_t)row[k + 1 + r];
+        __syncwarp();
+    } else {
+        nr = build_runs(ids, k, runs, lane);
+    }
     // split_long_runs (barle_compression.cpp:29-44), expanded in place from the back
     if (lane == 0) {
         int ns = 0;
