@@ -375,6 +375,22 @@ def make_scene(cfg: DsmConfig | str, heights: np.ndarray | None = None) -> Scene
                  float(z.max()), sun, dni, dhi, sl, asp)
 
 
+def scene_from_heightmap(name: str, heights: np.ndarray, voxel_size: float, lon: float, lat: float, tz: int,
+                         direct: np.ndarray | None = None, diffuse: np.ndarray | None = None, seed: int = 1) -> Scene:
+    """The inputs the reference CLI builds from a heightmap (src/main.cpp:70-127):
+    voxelization with the raster's pixel size, the sun series of the site,
+    and the given hourly TMY series (the seeded synthetic series when none
+    are given)."""
+    z = np.asarray(heights, np.float32)
+    H, W = z.shape
+    num_total, num_top, pp, wz, sl, asp = voxelize(z, voxel_size)
+    sun = sun_positions(lon, lat, tz)
+    if direct is None or diffuse is None:
+        direct, diffuse = make_tmy(sun, seed + 7)
+    return Scene(name, z.ravel().copy(), W, H, num_total, num_top, pp, wz, float(z.max()), sun,
+                 np.asarray(direct, np.float32)[:8760], np.asarray(diffuse, np.float32)[:8760], sl, asp)
+
+
 def scene_from_arrays(name: str, d: dict, width: int, height: int) -> Scene:
     """Rebuilds a Scene from stored arrays (golden fixtures)."""
     grid = np.asarray(d["grid"], np.float32)

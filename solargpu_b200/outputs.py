@@ -63,3 +63,19 @@ def write_raster(path: str, scene, irradiance: np.ndarray) -> None:
     """Top voxels' annual irradiance as float32 [height][width] (.npy)."""
     irr = np.asarray(irradiance, np.float32)
     np.save(path, irr[: scene.num_top].reshape(scene.height, scene.width))
+
+
+def write_geotiff(path: str, scene, irradiance: np.ndarray, meta=None) -> None:
+    """Top voxels' annual irradiance as a single-band float32 GeoTIFF, with the
+    input heightmap's georeferencing and compression when it came from one
+    (src/main.cpp:178, src/geotiff_io.cpp:157-185), else pixel size 1 and
+    no compression."""
+    from solargpu_b200 import geotiff
+    import dataclasses
+    m = dataclasses.replace(meta) if meta is not None else geotiff.TiffMeta(pixel_scale=[1.0, 1.0, 0.0],
+                                                                             tiepoints=[0.0] * 6)
+    m.w, m.h = scene.width, scene.height
+    if m.rows_per_strip <= 0 or m.rows_per_strip > m.h:
+        m.rows_per_strip = m.h
+    irr = np.asarray(irradiance, np.float32)
+    geotiff.write_tiff(path, irr[: scene.num_top].reshape(scene.height, scene.width), m)

@@ -18,9 +18,15 @@ code, compiled from its sources by oracle/Makefile:
                           CSR ids, ba-RLE sizes and bytes and shadow bitmap, plus a
                           digest of the generated scene's arrays
 
+  tiff   (this container: the reference tree and PIL)
+    ref_dsm_tiff.json     the reference's test heightmap (test_data/dsm_heightmap.tiff:
+                          tiled, Deflate, floating-point predictor) as decoded by PIL
+                          (libtiff): shape, SHA-256 of the float32 heights, GeoTIFF tags
+
     python tests/golden/make_golden.py host
     python tests/golden/make_golden.py gpu [--out DIR]
     python tests/golden/make_golden.py gpu-large [--out DIR]
+    python tests/golden/make_golden.py tiff
 """
 from __future__ import annotations
 
@@ -166,14 +172,34 @@ def gpu_large(out_dir: str, name: str = "dsm1024"):
     print(name, "blocks", len(dig), "nnz", r["csr_ids"].size, "barle bytes", r["barle"].size)
 
 
+def tiff():
+    import json
+    from PIL import Image
+    ref = os.environ.get("SOLARGPU_REFERENCE", "/root/reference")
+    path = os.path.join(ref, "test_data", "dsm_heightmap.tiff")
+    im = Image.open(path)
+    a = np.array(im, dtype=np.float32)
+    tags = im.tag_v2
+    out = {"file": "test_data/dsm_heightmap.tiff", "shape": list(a.shape), "sha256_float32": sha(a),
+           "min": float(a.min()), "max": float(a.max()),
+           "pixel_scale": list(tags.get(33550, ())), "tiepoints": list(tags.get(33922, ())),
+           "nodata": str(tags.get(42113, "")), "compression": int(tags.get(259, 1)),
+           "predictor": int(tags.get(317, 1)), "tile": [int(tags.get(322, 0)), int(tags.get(323, 0))]}
+    with open(os.path.join(HERE, "ref_dsm_tiff.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print(out)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["host", "gpu", "gpu-large"])
+    ap.add_argument("what", choices=["host", "gpu", "gpu-large", "tiff"])
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     if a.what == "host":
         host()
     elif a.what == "gpu":
         gpu(a.out)
+    elif a.what == "tiff":
+        tiff()
     else:
         gpu_large(a.out)
