@@ -44,14 +44,16 @@ enum { SOLAR_GPU_CSR = 0, SOLAR_GPU_BARLE = 1, SOLAR_GPU_BOTH = 2 };
 /* Annual accumulation. */
 enum { SOLAR_GPU_ACC_FP64 = 0, SOLAR_GPU_ACC_KAHAN = 1, SOLAR_GPU_ACC_FP32 = 2 };
 /* Reflection evaluation. */
-enum { SOLAR_GPU_REFL_HOURLY = 0, SOLAR_GPU_REFL_ANNUAL = 1 };
+enum { SOLAR_GPU_REFL_HOURLY = 0, SOLAR_GPU_REFL_ANNUAL = 1, SOLAR_GPU_REFL_NONE = 2 };
 
 typedef struct solar_gpu_options {
     int neighbor_format;     /* SOLAR_GPU_CSR / SOLAR_GPU_BARLE (SOLAR_GPU_BOTH: trace only) */
     int hour_block;          /* 1 = plain per-hour path; 32..512 = hour-block width (powers of 2); 0 = 128 */
     int accumulation;        /* SOLAR_GPU_ACC_* */
-    int reflection;          /* SOLAR_GPU_REFL_HOURLY (reflection per hour, reference semantics) or
-                                SOLAR_GPU_REFL_ANNUAL (sum over hours first, one sparse product) */
+    int reflection;          /* SOLAR_GPU_REFL_HOURLY (reflection per hour, reference semantics),
+                                SOLAR_GPU_REFL_ANNUAL (sum over hours first, one sparse product) or
+                                SOLAR_GPU_REFL_NONE (each voxel's own direct + diffuse only, FP64
+                                sums: the reflected share is 1 - none / hourly) */
     long long chunk_voxels;  /* tracer chunk in voxels (bounds the raw hit buffer); 0 = from free memory */
     int use_graph;           /* capture the hour-block loop in a CUDA graph */
     int time_kernels;        /* record CUDA events around every kernel group (no graph); see

@@ -26,7 +26,7 @@ HOURS_PER_YEAR = 8760
 
 CSR, BARLE, BOTH = 0, 1, 2
 ACC_FP64, ACC_KAHAN, ACC_FP32 = 0, 1, 2
-REFL_HOURLY, REFL_ANNUAL = 0, 1
+REFL_HOURLY, REFL_ANNUAL, REFL_NONE = 0, 1, 2
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no CUDA device",
            -4: "out of device memory", -5: "device data check failed"}

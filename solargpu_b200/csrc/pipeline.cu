@@ -263,7 +263,7 @@ int check_options(const solar_gpu_options* o, bool trace_only)
     if (!(B == 0 || B == 1 || B == 32 || B == 64 || B == 128 || B == 256 || B == 512))
         return fail(SOLAR_GPU_ERR_ARG, "hour_block %d (1, 32, 64, 128, 256 or 512)", B);
     if (o->accumulation < 0 || o->accumulation > 2) return fail(SOLAR_GPU_ERR_ARG, "accumulation %d", o->accumulation);
-    if (o->reflection < 0 || o->reflection > 1) return fail(SOLAR_GPU_ERR_ARG, "reflection %d", o->reflection);
+    if (o->reflection < 0 || o->reflection > 2) return fail(SOLAR_GPU_ERR_ARG, "reflection %d", o->reflection);
     if (o->chunk_voxels < 0) return fail(SOLAR_GPU_ERR_ARG, "chunk_voxels %lld", o->chunk_voxels);
     // hour-block widths each reflection kernel is built for
     const int V = o->group_size;
@@ -571,6 +571,20 @@ int stage23(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sc
     const uint32_t* sh = as<uint32_t>(c->shadow);
     const HourEntry* tab = as<HourEntry>(c->table);
     int* err = as<int>(c->err);
+    if (o->reflection == SOLAR_GPU_REFL_NONE) {
+        // own direct + diffuse only: the annual form's FP64 sums, no reflection
+        RK(ensure(c, c->sums, sizeof(double) * (size_t)N));
+        {
+            KScope k(c, SOLAR_GPU_KT_SOLAR);
+            CK(launch_solar_sum(g, N, sh, c->words32, tab, Hd, as<double>(c->sums), st));
+        }
+        {
+            KScope k(c, SOLAR_GPU_KT_FINALIZE);
+            CK(launch_finalize_f64(as<double>(c->sums), N, out, st));
+        }
+        c->launches += 2;
+        return SOLAR_GPU_OK;
+    }
     if (o->reflection == SOLAR_GPU_REFL_ANNUAL) {
         RK(ensure(c, c->sums, sizeof(double) * (size_t)N));
         RK(ensure(c, c->out_f64, sizeof(double) * (size_t)N));

@@ -1,7 +1,9 @@
 """Sky-bin visibility surrogate: a BF16 conv net on the tcgen05 GEMM.
 
 For a voxel, the model predicts its 265 sun-bin shadow bits (the DDA's
-shadow words: 1 = a ray toward that bin hits terrain).  Two inputs:
+shadow words: 1 = a ray toward that bin hits terrain) and its reflected
+irradiance share (the part of its annual irradiance that inter-reflection
+adds: 1 - own / total, own = the run with reflection=none).  Two inputs:
 
 * conv model (the default): a 64 x 64 x 2 image around the voxel, channel 0
   the 1 m cell heights, channel 1 the maxima of 8 x 8-cell context cells
@@ -13,7 +15,10 @@ shadow words: 1 = a ray toward that bin hits terrain).  Two inputs:
 * MLP model (`conv=None`): the 64 x 64 heights and the normal, zero-padded
   to 4224 columns, into the same MLP.
 
-The first `active` logits are the sun bins; ReLU between layers.  Every
+The first `active` logits are the sun bins, the next `share_units` (16) all
+learn the reflected share (soft binary cross-entropy targets; the prediction
+is the mean of their sigmoids, which gives the one scalar the weight of 16
+bins in the loss); ReLU between layers.  Every
 product, forward and backward, runs on the tensor cores through
 `solar_gpu_gemm_bf16` (bf16 operands, f32 accumulation in TMEM); a
 convolution is im2col + GEMM, its input gradient GEMM + col2im (fused with
@@ -25,8 +30,8 @@ moments are FP32, the GEMMs read bf16 copies.
 model, then per 256 x 256-cell tile a random sample of voxels traced exactly
 (`solar_gpu_trace_shadow_subset`); a tile whose sampled bit error exceeds the
 threshold (2%) is traced exactly in full.  The result is exact on fallback
-tiles and within the sampled error elsewhere.  The model does not predict the
-reflected share; reflection needs the exact neighbor lists.
+tiles and within the sampled error elsewhere.  The share is a preview only:
+the exact irradiance needs the exact neighbor lists.
 """
 from __future__ import annotations
 
@@ -98,11 +103,15 @@ class Surrogate:
     (W [Cout][Kp], Kp = 16 Cin rounded up to 128) then the MLP layers."""
 
     def __init__(self, active: int, hidden: int = 512, layers: int = 3, feat: int = FEAT, outw: int = OUTW,
-                 seed: int = 0, device: int = 0, conv: tuple | None = CONV):
+                 seed: int = 0, device: int = 0, conv: tuple | None = CONV, share_units: int = 16):
         import torch
         self.torch = torch
         self.dev = torch.device("cuda", device)
         self.active, self.outw = active, outw
+        if active + share_units > outw:
+            raise ValueError(f"{active} sun bins + {share_units} share units exceed {outw} outputs")
+        self.share_units = share_units
+        self.loss_cols = active + share_units
         self.conv = tuple(conv) if conv else ()
         g = torch.Generator(device="cpu").manual_seed(seed)
         self.W, self.b = [], []
@@ -162,12 +171,16 @@ class Surrogate:
         """Flat features of the MLP model."""
         return self.inputs(scene, dev, voxels)[0]
 
-    def labels(self, shadow_dev, words32: int, voxels):
+    def labels(self, shadow_dev, words32: int, voxels, share=None):
+        """Bit targets of the sun bins and, when `share` (per voxel, on the
+        device) is given, the reflected share in the share units."""
         torch = self.torch
         M = voxels.numel()
         y = torch.empty(M, self.outw, dtype=torch.float32, device=self.dev)
         api._check(_lib().solar_gpu_sg_labels(_p(shadow_dev), words32, _p(voxels), M, self.active, self.outw,
                                               _p(y), None))
+        if share is not None and self.share_units:
+            y[:, self.active:self.loss_cols] = share[voxels.long()].unsqueeze(1)
         return y
 
     # -- model ----------------------------------------------------------------
@@ -214,7 +227,7 @@ class Surrogate:
         ins, outs, Z = self.forward(X, nrm)
         loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
         g = torch.empty(B, self.outw, dtype=torch.bfloat16, device=self.dev)
-        api._check(L.solar_gpu_sg_bce(_p(Z), _p(Y), B, self.outw, self.active, _p(g), _p(loss), None))
+        api._check(L.solar_gpu_sg_bce(_p(Z), _p(Y), B, self.outw, self.loss_cols, _p(g), _p(loss), None))
         nc = len(self.conv)
         dW = [None] * len(self.W)
         db = [None] * len(self.W)
@@ -256,16 +269,16 @@ class Surrogate:
                                            self.b[l].numel(), lr, b1, b2, eps, self.step_count, None, None))
 
     def train(self, data: list, steps: int, batch: int = 1024, lr: float = 1e-3, seed: int = 0, log_every: int = 0):
-        """data: (scene, dev arrays, shadow words on the device, words32) per
-        training scene; batches of `batch` voxels (a multiple of 128) drawn
-        uniformly."""
+        """data: (scene, dev arrays, shadow words on the device, words32[,
+        reflected share per voxel on the device]) per training scene; batches
+        of `batch` voxels (a multiple of 128) drawn uniformly."""
         torch = self.torch
         rng = np.random.default_rng(seed)
         losses = []
         for it in range(steps):
-            scene, dev, shadow, words32 = data[it % len(data)]
+            scene, dev, shadow, words32, *rest = data[it % len(data)]
             vox = torch.from_numpy(rng.integers(0, scene.num_total, batch, dtype=np.int32)).to(self.dev)
-            Y = self.labels(shadow, words32, vox)
+            Y = self.labels(shadow, words32, vox, rest[0] if rest else None)
             inp = self.inputs(scene, dev, vox)
             loss, dW, db = self.gradients(inp[0], Y, *inp[1:])
             self.apply(dW, db, lr)
@@ -273,6 +286,22 @@ class Surrogate:
             if log_every and (it + 1) % log_every == 0:
                 print(f"step {it + 1}: loss {np.mean(losses[-log_every:]):.4f}", flush=True)
         return losses
+
+    def predict_share(self, scene, dev: dict, voxels, batch: int | None = None):
+        """Predicted reflected share per voxel (float32, on the device)."""
+        torch = self.torch
+        batch = batch or (4096 if self.conv else 16384)
+        n = voxels.numel()
+        out = torch.zeros(n, dtype=torch.float32, device=self.dev)
+        for i0 in range(0, n, batch):
+            v = voxels[i0:i0 + batch]
+            m = v.numel()
+            pad = (-m) % 128
+            if pad:
+                v = torch.cat([v, v[:1].expand(pad)])
+            _, _, Z = self.forward(*self.inputs(scene, dev, v))
+            out[i0:i0 + m] = torch.sigmoid(Z[:m, self.active:self.loss_cols]).mean(1)
+        return out
 
     def predict_bits(self, scene, dev: dict, voxels, batch: int | None = None):
         """Predicted shadow words [n][ceil(active/32)] (uint32, on the device)."""
@@ -381,13 +410,24 @@ def main(argv=None) -> int:
              "slopes": torch.from_numpy(s.slopes).cuda(), "aspects": torch.from_numpy(s.aspects).cuda()}
         return s, d
 
+    def share_of(ctx, s, d):
+        """1 - own / total per voxel: the reflected share of the annual irradiance."""
+        tot = torch.zeros(s.num_total, dtype=torch.float32, device="cuda")
+        own = torch.zeros_like(tot)
+        ctx.run_device(s, d, tot, neighbor_format=0)
+        ctx.run_device(s, d, own, neighbor_format=0, reflection=api.REFL_NONE)
+        return (1.0 - own.double() / tot.double().clamp_min(1.0)).clamp_min(0.0).float()
+
     res = {}
     with api.Context(0) as ctx:
         data = []
+        shares = []
         for name in a.train.split(","):
             s, d = staged(name)
+            share = share_of(ctx, s, d)
             r = ctx.trace(s, d, neighbor_format=0)
-            data.append((s, d, torch.from_numpy(r["shadow"].view(np.int32)).cuda(), r["shadow_words"]))
+            data.append((s, d, torch.from_numpy(r["shadow"].view(np.int32)).cuda(), r["shadow_words"], share))
+            shares.append(share)
             active = r["active_bins"]
         model = Surrogate(active=active, seed=0, conv=CONV if a.model == "conv" else None)
         t0 = time.perf_counter()
@@ -409,13 +449,29 @@ def main(argv=None) -> int:
         torch.cuda.synchronize()
         t_pred = time.perf_counter() - t0
         guarded = predict_with_fallback(model, ctx, s, d, max_err=a.max_err)
+        share_true = share_of(ctx, s, d)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        share_pred = model.predict_share(s, d, allv)
+        torch.cuda.synchronize()
+        t_share = time.perf_counter() - t0
+        err = (share_pred - share_true).abs()
+        mean_train = float(torch.cat(shares).mean())
+        base = (share_true - mean_train).abs()
         res["test"] = {"scene": a.test, "voxels": s.num_total, "active_bins": active,
                        "exact_trace_s": round(t_exact, 4), "model_only_s": round(t_pred, 4),
                        "model_bit_error": bit_error(pred, exact, active),
                        "guarded_s": round(guarded["total_s"], 4),
                        "guarded_bit_error": bit_error(guarded["words"], exact, active),
                        "tiles": len(guarded["tiles"]),
-                       "fallback_tiles": sum(t["fallback"] for t in guarded["tiles"])}
+                       "fallback_tiles": sum(t["fallback"] for t in guarded["tiles"]),
+                       "reflected_share": {"mean": float(share_true.mean()), "max": float(share_true.max()),
+                                           "model_abs_error_mean": float(err.mean()),
+                                           "model_abs_error_p99": float(err.quantile(0.99)) if err.numel() <= 1 << 24
+                                           else None,
+                                           "model_abs_error_max": float(err.max()),
+                                           "training_mean_abs_error_mean": float(base.mean()),
+                                           "model_only_s": round(t_share, 4)}}
         res["gemm"] = _gemm_stats(8192, 8192, 4096)
     print(json.dumps(res))
     return 0

@@ -186,6 +186,24 @@ def test_annual_form_vs_fp64(ctx, scene160, fmt):
     assert e.max() <= REL_TOL, (e.max(), e.mean())
 
 
+def test_own_irradiance_without_reflection_vs_fp64(ctx, scene160):
+    """reflection=none: each voxel's own direct + diffuse (the FP64 oracle's
+    second sum); the reflected share is 1 - own / total."""
+    import torch
+    from oracle import oracle as O
+    s = scene160
+    bins, off, ids, sh = oracle_trace(s)
+    tot, own = O.annual_fp64(s, sh, off, ids)
+    out = torch.zeros(s.num_total, dtype=torch.float32, device="cuda:0")
+    ctx.run_device(s, device_arrays(s), out, neighbor_format=0, reflection=2)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    e = rel_err(got, own)
+    assert e.max() <= REL_TOL, (e.max(), e.mean())
+    share = 1.0 - own / tot
+    assert share.min() >= 0.0 and share.max() > 0.0   # reflection only adds
+
+
 @pytest.mark.parametrize("fmt,V", [(0, 0), (1, 0), (0, 8), (1, 8), (1, 4), (0, 1), (1, 2), (0, 64), (1, 64)])
 def test_hour_block_vs_fp64_dsm160(ctx, scene160, fmt, V):
     import torch

@@ -71,7 +71,7 @@ def test_surrogate_gradients_match_fp64():
     import torch
     from solargpu_b200 import surrogate as S
     M, active = 128, 100
-    m = S.Surrogate(active=active, hidden=128, layers=1, feat=128, outw=128, seed=3, conv=None)
+    m = S.Surrogate(active=active, hidden=128, layers=1, feat=128, outw=128, seed=3, conv=None, share_units=0)
     g = torch.Generator(device="cpu").manual_seed(7)
     X = torch.randn(M, 128, generator=g).to(torch.bfloat16).cuda()
     Y = (torch.rand(M, 128, generator=g) > 0.5).float().cuda()
@@ -135,7 +135,7 @@ def test_conv_surrogate_gradients_match_fp64():
     import torch
     from solargpu_b200 import surrogate as S
     B, active = 128, 100
-    m = S.Surrogate(active=active, hidden=128, layers=1, outw=128, seed=5, conv=(64, 64))
+    m = S.Surrogate(active=active, hidden=128, layers=1, outw=128, seed=5, conv=(64, 64), share_units=0)
     assert m.feat == 16 * 16 * 64 + S.NRM and m.kp == [128, 1024]
     g = torch.Generator(device="cpu").manual_seed(11)
     img = torch.randn(B, 64, 64, 2, generator=g).to(torch.bfloat16).cuda()
@@ -246,3 +246,34 @@ def test_surrogate_learns_and_fallback_is_exact():
         for t in res["tiles"]:
             if t["sampled_error"] > 0:
                 assert t["fallback"]
+
+
+@pytest.mark.gpu
+def test_surrogate_learns_the_reflected_share():
+    """The share units: targets 1 - own / total from the pipeline's runs with
+    and without reflection, soft cross-entropy; a short training run brings
+    the predicted share of the scene's voxels closer to the exact one."""
+    import numpy as np
+    import torch
+    from conftest import device_arrays, load_scene
+    from solargpu_b200 import api
+    from solargpu_b200 import surrogate as S
+    s = load_scene("dsm64")
+    dev = device_arrays(s)
+    with api.Context(0) as ctx:
+        tot = torch.zeros(s.num_total, dtype=torch.float32, device="cuda")
+        own = torch.zeros_like(tot)
+        ctx.run_device(s, dev, tot, neighbor_format=0)
+        ctx.run_device(s, dev, own, neighbor_format=0, reflection=api.REFL_NONE)
+        share = (1.0 - own / tot).clamp_min(0.0)
+        assert float(share.max()) > 0.0 and float(share.min()) >= 0.0
+        r = ctx.trace(s, dev, neighbor_format=0)
+        sh = torch.from_numpy(r["shadow"].view(np.int32)).cuda()
+        m = S.Surrogate(active=r["active_bins"], seed=2, conv=None)
+        allv = torch.arange(s.num_total, dtype=torch.int32, device="cuda")
+        before = float((m.predict_share(s, dev, allv) - share).abs().mean())
+        m.train([(s, dev, sh, r["shadow_words"], share)], steps=150, batch=256, lr=1e-3)
+        p = m.predict_share(s, dev, allv)
+        after = float((p - share).abs().mean())
+        assert p.shape == (s.num_total,) and float(p.min()) >= 0.0 and float(p.max()) <= 1.0
+        assert after < 0.5 * before, (before, after)
