@@ -27,7 +27,7 @@ namespace sgb {
 namespace {
 
 constexpr int kTraceBlock = 128;
-constexpr int kDirParts = 16;      // blocks per voxel block, each a sixteenth of the directions
+constexpr int kDirParts = 32;      // blocks per voxel block, each 1/32 of the directions (16: +0.6% at 1024^2)
 constexpr int kDedupeWarps = 4;
 constexpr int kHashSlots = 4096;   // > 2592 possible distinct hits per voxel
 constexpr int kDedupeBatch = 9;    // 2592 = 9 batches of 9 rounds of 32 directions
