@@ -22,7 +22,7 @@ OUT = os.path.join(PKG, "_lib")
 OBJ = os.path.join(OUT, "obj")
 LIB = os.path.join(OUT, "libsolargpu_b200.so")
 
-CU_SOURCES = ["trace.cu", "barle.cu", "solar.cu", "reflect.cu", "group.cu", "tile.cu", "mma.cu", "voxel.cu",
+CU_SOURCES = ["trace.cu", "cone.cu", "barle.cu", "solar.cu", "reflect.cu", "group.cu", "tile.cu", "mma.cu", "voxel.cu",
               "pipeline.cu", "noalloc.cu", "surrogate.cu"]
 CXX_SOURCES = ["sky.cpp", "cxx_api.cpp"]
 HEADERS = ["sgb_internal.cuh", "solar_math.cuh", "sky.h"]

@@ -10,8 +10,10 @@
 //     CSR and/or ba-RLE lists on the device (no host round trip of the raw
 //     hit buffer, no host encoder);
 //   * errors come back as return codes, never exit().
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -111,7 +113,7 @@ struct solar_gpu_context {
         grp_cell, grp_w, w_cnt, w_off, w_tmp, w_cell, w_val, order_first, order_inv, tile_flag, tile_pos,
         tile_start, tile_union, tile_slot, tile_rows, tile_gcnt, tile_gnch, tile_gbase, tile_tbase, tile_table,
         tile_erow, tile_ew, chunk_perm, chunk_flag, chunk_pos, chunk_tmp, mma_union, mma_nch, mma_cbase,
-        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp, gpad, mma_sched, mma_retry;
+        mma_ccnt, mma_coff, mma_ent, mma_scale, mma_over, slab16, dd_ovf, vox_cnt, vox_off, vox_tmp, gpad, mma_sched, mma_retry, cone, cone_tmp, cone_specs;
     int* h_scalars = nullptr;   // pinned host scratch for small read-backs
     long long mem_limit = 0;    // device bytes the buffers may hold (0: no limit)
     size_t dev_total = 0;       // device memory size, read once at creation
@@ -139,7 +141,7 @@ struct solar_gpu_context {
     cudaStream_t kt_stream = nullptr;
 };
 
-static constexpr int kNumBufs = 81;
+static constexpr int kNumBufs = 84;
 extern "C" {
 static void all_bufs(solar_gpu_context* c, DevBuf** out);   // defined with the exports below
 }
@@ -296,6 +298,8 @@ DevScene dev_scene(const solar_gpu_scene* s)
     d.N = s->num_total_voxels;
     d.T = s->num_top_voxels;
     d.maxz = s->max_height;
+    d.cone = nullptr;
+    d.cone_stride = 0;
     return d;
 }
 
@@ -382,14 +386,47 @@ long long auto_chunk(solar_gpu_context* c, int N, int D)
     return chunk;
 }
 
-// The tracer's copy of the heightmap inside a border of +inf (one pass over
-// the grid, rebuilt each call: the caller may change heights between calls).
-int padded_grid(solar_gpu_context* c, const solar_gpu_scene* s, DevScene& ds, cudaStream_t st)
+// The tracer's copy of the heightmap inside a border of +inf and the
+// early-exit tables of the upper directions (cone.cu), rebuilt each call (the
+// caller may change heights between calls).  The tables and their scratch
+// may take a quarter of the free device memory (and of what a memory limit
+// leaves); past that, or with SGB_CONE=0, the tracer runs without them (the
+// reference's range test alone).
+int padded_grid(solar_gpu_context* c, const solar_gpu_scene* s, const SkyTables& sky, DevScene& ds,
+                cudaStream_t st)
 {
-    RK(ensure(c, c->gpad, sizeof(float) * (size_t)(s->grid_width + 2) * (size_t)(s->grid_height + 2)));
-    CK(launch_pad_grid(s->grid, s->grid_width, s->grid_height, as<float>(c->gpad), st));
-    c->launches += 1;
+    const int W = s->grid_width, H = s->grid_height;
+    const size_t cells = (size_t)(W + 2) * (size_t)(H + 2);
+    RK(ensure(c, c->gpad, sizeof(float) * cells));
+    CK(launch_pad_grid(s->grid, W, H, as<float>(c->gpad), st));
+    int nt = (int)sky.cones.size();
+    if (const char* env = std::getenv("SGB_CONE"))
+        if (std::atoi(env) == 0) nt = 0;
+    const size_t bytes = sizeof(float) * cells * (size_t)nt;
+    if (nt > 0 && (c->cone.cap < bytes || c->cone_tmp.cap < bytes)) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+        size_t room = free_b + c->cone.cap + c->cone_tmp.cap;
+        if (c->mem_limit > 0) {
+            const size_t held = held_bytes(c) - c->cone.cap - c->cone_tmp.cap;
+            room = std::min(room, (size_t)c->mem_limit > held ? (size_t)c->mem_limit - held : (size_t)0);
+        }
+        if (2 * bytes > room / 4) nt = 0;
+    }
     ds.gpad = as<float>(c->gpad);
+    ds.cone = nullptr;
+    ds.cone_stride = 0;
+    c->launches += 1;
+    if (nt == 0) return SOLAR_GPU_OK;
+    RK(ensure(c, c->cone, bytes));
+    RK(ensure(c, c->cone_tmp, bytes));
+    RK(ensure(c, c->cone_specs, sizeof(ConeSpec) * nt));
+    CK(cudaMemcpyAsync(c->cone_specs.p, sky.cones.data(), sizeof(ConeSpec) * nt, cudaMemcpyHostToDevice, st));
+    CK(launch_cone_tables(s->grid, W, H, s->max_height, as<ConeSpec>(c->cone_specs), nt, as<float>(c->cone),
+                          as<float>(c->cone_tmp), cells, st));
+    c->launches += 5;
+    ds.cone = as<float>(c->cone);
+    ds.cone_stride = cells;
     return SOLAR_GPU_OK;
 }
 
@@ -422,7 +459,10 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
         RK(ensure(c, c->barle_bytes, (size_t)N * 160));
     }
     DevScene ds = dev_scene(s);
-    RK(padded_grid(c, s, ds, st));
+    {
+        KScope k(c, SOLAR_GPU_KT_TRACE);   // the tracer's inputs count with the tracer
+        RK(padded_grid(c, s, sky, ds, st));
+    }
     // Rows follow the visiting order (Morton-adjacent voxels share a warp, so
     // their rays have similar lengths); with several chunks, each chunk (a
     // range of voxel indices) is traced in the visiting order of its voxels.
@@ -510,9 +550,11 @@ int stage1(solar_gpu_context* c, const solar_gpu_options* o, const solar_gpu_sce
     // smaller ones are kept for the next call.
     if (c->raw.cap > c->dev_total / 4) {
         c->squeezed = true;
-        CK(cudaFree(c->raw.p));
-        c->raw.p = nullptr;
-        c->raw.cap = 0;
+        for (DevBuf* b : {&c->raw, &c->cone, &c->cone_tmp}) {
+            CK(cudaFree(b->p));
+            b->p = nullptr;
+            b->cap = 0;
+        }
     }
     return SOLAR_GPU_OK;
 }
@@ -1092,7 +1134,7 @@ int trace_subset_impl(solar_gpu_context* c, const solar_gpu_scene* s, const int*
     std::memcpy(&bad, c->h_scalars, sizeof(int));
     if (bad) return fail(SOLAR_GPU_ERR_ARG, "voxel ids outside [0, %d)", N);
     DevScene ds = dev_scene(s);
-    RK(padded_grid(c, s, ds, st));
+    RK(padded_grid(c, s, sky, ds, st));
     CK(launch_trace(ds, as<DirEntry>(c->dirs), D, words32, 0, n, as<int>(c->raw),
                     as<uint32_t>(c->shadow), voxels, as<int>(c->err), st));
     const long long cells = (long long)n * words32;
@@ -1192,7 +1234,8 @@ static void all_bufs(solar_gpu_context* c, DevBuf** out)
                                 &c->tile_table, &c->tile_erow, &c->tile_ew, &c->chunk_perm, &c->chunk_flag,
                                 &c->chunk_pos, &c->chunk_tmp, &c->mma_union, &c->mma_nch, &c->mma_cbase,
                                 &c->mma_ccnt, &c->mma_coff, &c->mma_ent, &c->mma_scale, &c->mma_over, &c->slab16,
-                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp, &c->gpad, &c->mma_sched, &c->mma_retry};
+                                &c->dd_ovf, &c->vox_cnt, &c->vox_off, &c->vox_tmp, &c->gpad, &c->mma_sched, &c->mma_retry,
+                                &c->cone, &c->cone_tmp, &c->cone_specs};
     for (int i = 0; i < kNumBufs; ++i) out[i] = bufs[i];
 }
 

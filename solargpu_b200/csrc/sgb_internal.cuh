@@ -29,8 +29,19 @@ struct DirEntry {
     float cx, cy, cz;
     float ax, ay;      // fmaxf(fabsf(c), 1e-8f)
     float dX, dY;      // 1.0f / ax, 1.0f / ay (IEEE)
-    int meta;          // bits 0..15: dense sun bin + 1 (0 = none); bit 16: upper hemisphere
+    int meta;          // bits 0..15: dense sun bin + 1 (0 = none); bit 16: upper hemisphere;
+                       // bits 17..26: early-exit table of an upper direction (cone.cu)
 };
+
+// The integer cone of one early-exit table (cone.cu): directions of quadrant
+// (sx, sy) whose unsigned step vector (1/dX, 1/dY) lies between the
+// primitive vectors a = (ax, ay) and b = (bx, by), det(a, b) = 1.
+struct ConeSpec {
+    int sx, sy;
+    int ax, ay, bx, by;
+};
+constexpr int kConeOrder = 8;        // cone vectors have components <= 8
+constexpr int kMaxConeTables = 1024; // 10 bits of DirEntry::meta
 
 // Per daylight hour, FP32 values of the FP64-evaluated solar geometry.
 //   cos_aoi(v) = dot(n_v, s)
@@ -52,6 +63,10 @@ struct DevScene {
     const float* aspects;     // [N]
     int W, H, N, T;
     float maxz;
+    // [tables][H + 2][W + 2] early-exit bounds of upper rays (cone.cu), or
+    // nullptr (no early exit: the reference's range test alone)
+    const float* cone;
+    size_t cone_stride;
 };
 
 // Per-voxel geometry derived once per call.
@@ -74,7 +89,12 @@ void set_last_error(const char* msg);
 // voxel), else chunk voxel lv; kernels that iterate voxels take the inverse.
 // gpad [(H + 2) * (W + 2)] = grid inside a one-cell border of +inf.
 cudaError_t launch_pad_grid(const float* grid, int W, int H, float* gpad, cudaStream_t st);
-// s.gpad must be set (launch_pad_grid).
+// Early-exit tables (cone.cu): n_specs bordered tables of `stride` floats in
+// tabs; tmp holds as many (scratch).
+cudaError_t launch_cone_tables(const float* grid, int W, int H, float maxz, const ConeSpec* specs, int n_specs,
+                               float* tabs, float* tmp, size_t stride, cudaStream_t st);
+int cone_window_radius(int W, int H);
+// s.gpad must be set (launch_pad_grid); s.cone may be nullptr.
 cudaError_t launch_trace(const DevScene& s, const DirEntry* dirs, int D, int words32,
                          int voxel_offset, int chunk_count, int* raw, uint32_t* shadow,
                          const int* perm, int* err, cudaStream_t st);

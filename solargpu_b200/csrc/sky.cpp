@@ -8,14 +8,49 @@
 //     over 72 azimuths, j-minor over 18 upper then 18 lower elevations,
 //     float cosf/sinf, normalised).
 // Compiled with -ffp-contract=off so no product is fused on the host.
+//
+// Each upper direction also names the early-exit table of its cone (cone.cu):
+// its quadrant and the two consecutive vectors of the Farey set of order
+// kConeOrder between which its unsigned step vector (1/dX, 1/dY) lies.
 #include "sky.h"
 
+#include <algorithm>
 #include <cmath>
+#include <map>
+#include <numeric>
+#include <tuple>
 
 namespace sgb {
 
 namespace {
 constexpr float kDegToRad = 0.0174532925f;   // include/pipeline_math_constants.h:15
+
+// Primitive vectors (p, q), 0 <= p, q <= n, by angle from (1, 0) to (0, 1);
+// consecutive ones have determinant 1.
+std::vector<std::pair<int, int>> farey_vectors(int n)
+{
+    std::vector<std::pair<int, int>> v;
+    for (int p = 0; p <= n; ++p)
+        for (int q = 0; q <= n; ++q)
+            if ((p || q) && std::gcd(p, q) == 1) v.emplace_back(p, q);
+    std::sort(v.begin(), v.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+        return (long long)a.first * b.second - (long long)a.second * b.first > 0;
+    });
+    return v;
+}
+
+// Index of the cone (F[k], F[k + 1]) holding the direction (dY, dX), which
+// is proportional to (1/dX, 1/dY).  The cross products of small integers
+// with floats are exact in double and so are their signs.
+int cone_of(const std::vector<std::pair<int, int>>& F, float dX, float dY)
+{
+    for (size_t k = 0; k + 1 < F.size(); ++k) {
+        const double a = (double)F[k].first * dX - (double)F[k].second * dY;             // det(F[k], v)
+        const double b = (double)dY * F[k + 1].second - (double)dX * F[k + 1].first;     // det(v, F[k+1])
+        if (a >= 0.0 && b >= 0.0) return (int)k;
+    }
+    return -1;
+}
 }
 
 SkyTables make_sky_tables(const float* sun_az_alt, float h_res, float v_res)
@@ -84,6 +119,33 @@ SkyTables make_sky_tables(const float* sun_az_alt, float h_res, float v_res)
             d.meta = ((dense + 1) & 0xFFFF) | (upper << 16);
         }
     }
+
+    // Every upper direction gets a table, or none does (the tracer then uses
+    // one table whose bound is maxz for all of them).
+    const std::vector<std::pair<int, int>> F = farey_vectors(kConeOrder);
+    bool ok = true;
+    for (size_t k = 0; k + 1 < F.size(); ++k)
+        ok = ok && (long long)F[k].first * F[k + 1].second - (long long)F[k].second * F[k + 1].first == 1;
+    std::map<std::tuple<int, int, int>, int> table_of;
+    std::vector<int> table(t.dirs.size(), 0);
+    for (size_t i = 0; ok && i < t.dirs.size(); ++i) {
+        const DirEntry& d = t.dirs[i];
+        if (!((d.meta >> 16) & 1)) continue;
+        const int sx = d.cx >= 0.0f ? 1 : -1, sy = d.cy >= 0.0f ? 1 : -1;
+        const int k = cone_of(F, d.dX, d.dY);
+        if (k < 0) { ok = false; break; }   // not reached: the cones cover the quadrant
+        const auto key = std::make_tuple(sx, sy, k);
+        auto it = table_of.find(key);
+        if (it == table_of.end()) {
+            if ((int)t.cones.size() >= kMaxConeTables) { ok = false; break; }
+            it = table_of.emplace(key, (int)t.cones.size()).first;
+            t.cones.push_back({sx, sy, F[k].first, F[k].second, F[k + 1].first, F[k + 1].second});
+        }
+        table[i] = it->second;
+    }
+    if (!ok) t.cones.clear();
+    else
+        for (size_t i = 0; i < t.dirs.size(); ++i) t.dirs[i].meta |= table[i] << 17;
     return t;
 }
 

@@ -16,6 +16,7 @@ struct SkyTables {
     std::vector<float> nudged;      // [8760 * 2]
     std::vector<int> hour_index;    // daylight hours (nudged altitude >= 1 deg), ascending
     std::vector<DirEntry> dirs;     // [hsize * vsize_full]
+    std::vector<ConeSpec> cones;    // early-exit tables named by the upper directions' meta
 };
 
 SkyTables make_sky_tables(const float* sun_az_alt, float h_res = 5.0f, float v_res = 5.0f);

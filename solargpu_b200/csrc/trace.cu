@@ -17,7 +17,10 @@
 //     separate warp-per-voxel pass with a shared-memory hash set and
 //     ballot/popc compaction that keeps direction order;
 //   * shadow bits are packed 32 per word, voxel-major ([N][words32]), and
-//     written once per word.
+//     written once per word;
+//   * an upper ray also ends, with no hit, once it rises above every cell it
+//     can still reach (the early-exit tables of cone.cu): the reference's
+//     result with fewer steps.
 #include "sgb_internal.cuh"
 
 #include <algorithm>
@@ -37,12 +40,36 @@ constexpr int kDedupeBatch = 9;    // 2592 = 9 batches of 9 rounds of 32 directi
 // steps off the grid meets the border, whose height test is always true, so
 // the loop needs no per-axis step counts; the cell it stopped on tells a
 // border stop (no hit, as the reference's bounds check) from a hit.  Heights
-// inside the grid are the caller's, +inf included.  One unsigned compare a
-// step keeps every load inside the copy whatever the float tests do; it
-// never ends a ray (the border does first) and returns -1 if it did.
-template <bool UP>
-__device__ __forceinline__ int trace_ray(const float* __restrict__ gpad, int W, int H, float maxz, int gx, int gy,
-                                         float base_z, const DirEntry& d)
+// inside the grid are the caller's, +inf included.  Each load's index is
+// clamped into the copy (one unsigned min a step), so every load stays inside
+// it whatever the float tests do; a ray never leaves the copy (the border
+// ends it first), and one that did would end on the clamped border cell and
+// return -1.  (The clamp measured 2.7% faster than a compare and branch.)
+//
+// With CONE, an upper ray also reads its direction's early-exit table
+// (cone.cu) every kBoundEvery steps: a ray above the bound of a cell it has
+// passed can hit nothing from there on (every later cell is reachable from
+// that cell), so it ends with no hit, as the reference's range test would
+// end it or as it would leave the grid.  (Reading the bound every step,
+// packed with the height, cost more in loads than the steps it saved.)
+constexpr int kBoundEvery = 8;    // steps between bound checks (4: +5.7%, 6: +1.6% at 1024^2)
+
+__device__ __forceinline__ void dda_step(float& t, float& tMaxX, float& tMaxY, int& cell, int sx, int step_y,
+                                         const DirEntry& d)
+{
+    // one step, as selects: lanes that step on different axes stay
+    // converged (measured 119.6 -> 116.5 ms at 1024^2 against branches)
+    const bool xs = tMaxX < tMaxY;
+    t = fminf(tMaxX, tMaxY);   // = xs ? tMaxX : tMaxY (equal when not xs and equal)
+    cell += xs ? sx : step_y;
+    const float nx = __fadd_rn(tMaxX, d.dX), ny = __fadd_rn(tMaxY, d.dY);
+    tMaxX = xs ? nx : tMaxX;
+    tMaxY = xs ? tMaxY : ny;
+}
+
+template <bool UP, bool CONE>
+__device__ __forceinline__ int trace_ray(const float* __restrict__ gpad, const float* __restrict__ bound, int W,
+                                         int H, float maxz, int gx, int gy, float base_z, const DirEntry& d)
 {
     // Cdir * 2.0f is exact, so these match the reference fused or not.
     const float ox = __fadd_rn((float)gx, __fmul_rn(d.cx, 2.0f));
@@ -70,23 +97,33 @@ __device__ __forceinline__ int trace_ray(const float* __restrict__ gpad, int W, 
     const int Wp = W + 2;
     const int step_y = py ? Wp : -Wp;
     int cell = (ix + 1) + (iy + 1) * Wp;
-    const unsigned cells = (unsigned)Wp * (unsigned)(H + 2);
+    const unsigned last = (unsigned)Wp * (unsigned)(H + 2) - 1u;
     float zr;
-    for (;;) {
-        if ((unsigned)cell >= cells) return -1;
-        zr = __fmaf_rn(d.cz, t, oz);
-        // the reference tests the height range before the hit; both end the
-        // ray, and which one it was is decided once, after the loop
-        if ((UP ? (zr > maxz) : (zr < 0.0f)) || __fsub_rn(__ldg(gpad + cell), zr) > 0.01f) break;
-        // one step, as selects: lanes that step on different axes stay
-        // converged (measured 119.6 -> 116.5 ms at 1024^2 against branches)
-        const bool xs = tMaxX < tMaxY;
-        t = fminf(tMaxX, tMaxY);   // = xs ? tMaxX : tMaxY (equal when not xs and equal)
-        cell += xs ? sx : step_y;
-        const float nx = __fadd_rn(tMaxX, d.dX), ny = __fadd_rn(tMaxY, d.dY);
-        tMaxX = xs ? nx : tMaxX;
-        tMaxY = xs ? tMaxY : ny;
+    // the reference tests the height range before the hit; both end the ray,
+    // and which one it was is decided once, after the loop
+    if constexpr (CONE) {
+        for (;;) {
+            // The bound of the cell the group of steps starts on also bounds
+            // every cell after it, so its load has the whole group to arrive.
+            const float b = __ldg(bound + min((unsigned)cell, last));
+#pragma unroll
+            for (int k = 0; k < kBoundEvery; ++k) {
+                zr = __fmaf_rn(d.cz, t, oz);
+                if (zr > maxz || __fsub_rn(__ldg(gpad + min((unsigned)cell, last)), zr) > 0.01f) goto stopped;
+                dda_step(t, tMaxX, tMaxY, cell, sx, step_y, d);
+            }
+            if (__fmaf_rn(d.cz, t, oz) > b) return (unsigned)cell > last ? -1 : 0;
+        }
+    } else {
+        for (;;) {
+            zr = __fmaf_rn(d.cz, t, oz);
+            if ((UP ? (zr > maxz) : (zr < 0.0f)) || __fsub_rn(__ldg(gpad + min((unsigned)cell, last)), zr) > 0.01f)
+                goto stopped;
+            dda_step(t, tMaxX, tMaxY, cell, sx, step_y, d);
+        }
     }
+stopped:
+    if ((unsigned)cell > last) return -1;
     if (UP ? (zr > maxz) : (zr < 0.0f)) return 0;
     const int r = cell / Wp, q = cell - r * Wp;
     if (q == 0 || q > W || r == 0 || r > H) return 0;   // the border: the ray left the grid
@@ -122,10 +159,17 @@ k_trace(DevScene s, const DirEntry* __restrict__ dirs, int D, int words32,
     for (int g0 = gb * kRawGroup; g0 < ge * kRawGroup; g0 += kRawGroup) {
         for (int k = 0; k < kRawGroup; ++k) {
             const DirEntry d = dirs[g0 + k];
-            // up/down is the same for the whole warp (one direction at a time)
-            int hit = !active ? 0
-                      : ((d.meta >> 16) & 1) ? trace_ray<true>(s.gpad, s.W, s.H, s.maxz, gx, gy, base_z, d)
-                                             : trace_ray<false>(s.gpad, s.W, s.H, s.maxz, gx, gy, base_z, d);
+            // up/down and the table are the same for the whole warp (one direction at a time)
+            int hit = 0;
+            if (active) {
+                if (!((d.meta >> 16) & 1))
+                    hit = trace_ray<false, false>(s.gpad, nullptr, s.W, s.H, s.maxz, gx, gy, base_z, d);
+                else if (s.cone)
+                    hit = trace_ray<true, true>(s.gpad, s.cone + s.cone_stride * ((d.meta >> 17) & (kMaxConeTables - 1)),
+                                                s.W, s.H, s.maxz, gx, gy, base_z, d);
+                else
+                    hit = trace_ray<true, false>(s.gpad, nullptr, s.W, s.H, s.maxz, gx, gy, base_z, d);
+            }
             if (hit < 0) {
                 atomicOr(err, kErrTraceBounds);
                 hit = 0;

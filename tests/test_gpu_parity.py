@@ -71,6 +71,51 @@ def test_trace_nonfinite_heights_match_oracle(ctx):
     np.testing.assert_array_equal(r["shadow"], sh)
 
 
+@pytest.mark.parametrize("max_height", ["true", "below", "nan"])
+def test_trace_early_exit_on_towers_matches_oracle(ctx, max_height):
+    """Upper rays end early once they pass the early-exit bound of their cone
+    of directions (cone.cu).  A non-square field of low blocks with a few tall
+    towers, NaN and +inf cells, traced with the scene maximum as given, with a
+    maximum below the tallest tower (the reference's range test then ends rays
+    that would still hit it) and with a NaN maximum (the range test never
+    fires): lists and shadow bits equal the oracle's."""
+    import dataclasses
+    from oracle import oracle as O
+    from solargpu_b200 import inputs
+    rng = np.random.default_rng(7)
+    h = (rng.random((83, 117)) * 4.0).astype(np.float32)
+    for _ in range(40):
+        y, x = rng.integers(0, 80), rng.integers(0, 114)
+        h[y:y + rng.integers(1, 4), x:x + rng.integers(1, 4)] += np.float32(rng.random() * 25.0)
+    for y, x, v in [(5, 9, 60.0), (70, 100, 45.0), (41, 58, 52.0)]:
+        h[y, x] = v
+    s = inputs.scene_from_heightmap("towers", h, 1.0, 15.592, 46.543, 1)
+    g = s.grid.copy()
+    g[20 * 117 + 3], g[60 * 117 + 60] = np.nan, np.inf   # after voxelization, which wants finite heights
+    mz = {"true": s.max_height, "below": np.float32(30.0), "nan": np.float32(np.nan)}[max_height]
+    s = dataclasses.replace(s, name="towers_" + max_height, grid=g, max_height=mz)
+    bins, off, ids, sh = oracle_trace(s)
+    r = ctx.trace(s, device_arrays(s), neighbor_format=2)
+    np.testing.assert_array_equal(r["csr_off"], off)
+    np.testing.assert_array_equal(r["csr_ids"], ids)
+    np.testing.assert_array_equal(r["shadow"], sh)
+    boff, bbytes = O.barle_encode_csr(off, ids)
+    np.testing.assert_array_equal(r["barle_off"], boff)
+    np.testing.assert_array_equal(r["barle"], bbytes)
+
+
+def test_trace_without_early_exit_tables_gives_the_same_lists(ctx, scene160, monkeypatch):
+    """SGB_CONE=0 leaves one table whose bound is the scene maximum (the
+    reference's range test alone): the lists and shadow bits are the same
+    bits as with the cone tables."""
+    d = device_arrays(scene160)
+    a = ctx.trace(scene160, d, neighbor_format=2)
+    monkeypatch.setenv("SGB_CONE", "0")
+    b = ctx.trace(scene160, d, neighbor_format=2)
+    for k in ("csr_off", "csr_ids", "barle_off", "barle", "shadow"):
+        np.testing.assert_array_equal(a[k], b[k])
+
+
 def test_dedupe_second_pass_gives_the_same_lists(cuda_lib, scene160):
     """The first-occurrence dedupe first runs with small hash sets and hands
     the rows it gives up on to a second pass with large ones.  With the
