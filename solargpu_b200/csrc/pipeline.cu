@@ -132,6 +132,9 @@ struct solar_gpu_context {
     bool squeezed = false;
     // solar_gpu_run_batch: stage23 stops before the hour loop and leaves it here
     bool defer_hours = false;
+    // solar_gpu_run_batch: the early-exit tables of every tile are built in
+    // one buffer (the first context's), tile after tile on one stream
+    DevBuf* cone_shared = nullptr;
     HourLoop hours;
     // per kernel-group event log (time_kernels)
     bool ktime = false;
@@ -388,10 +391,13 @@ long long auto_chunk(solar_gpu_context* c, int N, int D)
 
 // The tracer's copy of the heightmap inside a border of +inf and the
 // early-exit tables of the upper directions (cone.cu), rebuilt each call (the
-// caller may change heights between calls).  The tables and their scratch
-// may take a quarter of the free device memory (and of what a memory limit
-// leaves); past that, or with SGB_CONE=0, the tracer runs without them (the
-// reference's range test alone).
+// caller may change heights between calls).  The tables' build scratch is the
+// raw hit buffer (not yet written: the tracer runs after the build) when it
+// is large enough.  New table memory may take a sixteenth of the free device
+// memory (and of what a memory limit leaves): the tables only save time, and
+// contexts of many tiles held at once leave little room; past that, or with
+// SGB_CONE=0, the tracer runs without them (the reference's range test
+// alone).
 int padded_grid(solar_gpu_context* c, const solar_gpu_scene* s, const SkyTables& sky, DevScene& ds,
                 cudaStream_t st)
 {
@@ -402,30 +408,38 @@ int padded_grid(solar_gpu_context* c, const solar_gpu_scene* s, const SkyTables&
     int nt = (int)sky.cones.size();
     if (const char* env = std::getenv("SGB_CONE"))
         if (std::atoi(env) == 0) nt = 0;
+    DevBuf& tabs = c->cone_shared ? *c->cone_shared : c->cone;
     const size_t bytes = sizeof(float) * cells * (size_t)nt;
-    if (nt > 0 && (c->cone.cap < bytes || c->cone_tmp.cap < bytes)) {
+    const bool scratch_in_raw = c->raw.cap >= bytes;
+    // device memory these tables would add to what the context holds
+    const size_t grow = (bytes > tabs.cap ? bytes - tabs.cap : 0) +
+                        (!scratch_in_raw && bytes > c->cone_tmp.cap ? bytes - c->cone_tmp.cap : 0);
+    if (nt > 0 && grow > 0) {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
-        size_t room = free_b + c->cone.cap + c->cone_tmp.cap;
+        size_t room = free_b;
         if (c->mem_limit > 0) {
-            const size_t held = held_bytes(c) - c->cone.cap - c->cone_tmp.cap;
+            const size_t held = held_bytes(c);
             room = std::min(room, (size_t)c->mem_limit > held ? (size_t)c->mem_limit - held : (size_t)0);
         }
-        if (2 * bytes > room / 4) nt = 0;
+        if (grow > room / 16) nt = 0;
     }
     ds.gpad = as<float>(c->gpad);
     ds.cone = nullptr;
     ds.cone_stride = 0;
     c->launches += 1;
     if (nt == 0) return SOLAR_GPU_OK;
-    RK(ensure(c, c->cone, bytes));
-    RK(ensure(c, c->cone_tmp, bytes));
+    if (ensure(c, tabs, bytes) != SOLAR_GPU_OK ||
+        (!scratch_in_raw && ensure(c, c->cone_tmp, bytes) != SOLAR_GPU_OK)) {
+        (void)cudaGetLastError();   // no room after all: the tracer runs without the tables
+        return SOLAR_GPU_OK;
+    }
     RK(ensure(c, c->cone_specs, sizeof(ConeSpec) * nt));
     CK(cudaMemcpyAsync(c->cone_specs.p, sky.cones.data(), sizeof(ConeSpec) * nt, cudaMemcpyHostToDevice, st));
-    CK(launch_cone_tables(s->grid, W, H, s->max_height, as<ConeSpec>(c->cone_specs), nt, as<float>(c->cone),
-                          as<float>(c->cone_tmp), cells, st));
+    CK(launch_cone_tables(s->grid, W, H, s->max_height, as<ConeSpec>(c->cone_specs), nt, as<float>(tabs),
+                          scratch_in_raw ? as<float>(c->raw) : as<float>(c->cone_tmp), cells, st));
     c->launches += 5;
-    ds.cone = as<float>(c->cone);
+    ds.cone = as<float>(tabs);
     ds.cone_stride = cells;
     return SOLAR_GPU_OK;
 }
@@ -1317,8 +1331,10 @@ int solar_gpu_run_batch(solar_gpu_context* const* ctxs, int n, const solar_gpu_o
         solar_gpu_options ob = opts[i];
         ob.time_kernels = 0;
         c->defer_hours = true;
+        c->cone_shared = &ctxs[0]->cone;   // one stream: tile i's tables are built after tile i - 1 is traced
         const int rc = run_device_impl(c, &ob, &scenes[i], outs[i], st, false);
         c->defer_hours = false;
+        c->cone_shared = nullptr;
         if (rc != SOLAR_GPU_OK) return rc;
     }
     // One CUDA graph holds every tile's hour loop as a branch of its own (on
