@@ -44,6 +44,7 @@
 // never hits and fmaxf skips it; +inf enters the maximum as itself.
 #include "sgb_internal.cuh"
 
+#include <climits>
 #include <cmath>
 
 namespace sgb {
@@ -79,8 +80,11 @@ __global__ void k_cone_lines(const float* __restrict__ src, int W, int H, const 
     else        { const long long k2 = k - n1; X = (int)(k2 % (W - uu)); Y = H - vv + (int)(k2 / (W - uu)); }
     const float* in = PASS == 0 ? src : src + stride * blockIdx.y;
     float* out = dst + stride * blockIdx.y;
+    // a known trip count lets the loads of an unrolled stretch issue together
+    const int n = min(u > 0 ? X / u : INT_MAX, v > 0 ? Y / v : INT_MAX) + 1;
     float m = -__int_as_float(0x7f800000);
-    for (; X >= 0 && Y >= 0; X -= u, Y -= v) {
+#pragma unroll 4
+    for (int i = 0; i < n; ++i, X -= u, Y -= v) {
         int x, y;
         to_grid(c, X, Y, W, H, x, y);
         const size_t p = pad_index(x, y, W);
@@ -90,28 +94,68 @@ __global__ void k_cone_lines(const float* __restrict__ src, int W, int H, const 
 }
 
 // Window maxima of M: PASS 0 over X offsets, PASS 1 over Y offsets (then
-// min with maxz); both read src and write dst (bordered tables).
+// min with maxz); both read src and write dst (bordered tables).  A block
+// stages the stretch of its rows (PASS 0: 256 cells of one row; PASS 1: 64
+// rows of 32 columns) plus the window's reach in shared memory, cells past
+// the grid as -inf (a window clipped at the grid's edge), and each cell
+// takes the maximum of its window from there.
+constexpr int kWinRow = 256;          // PASS 0: cells of a row per block
+constexpr int kWinCols = 32, kWinRows = 64, kWinRowsPerThread = 8;   // PASS 1 (256 threads)
+
 template <int PASS>
-__global__ void k_cone_window(int W, int H, float maxz, int r, const ConeSpec* __restrict__ specs,
-                              const float* __restrict__ src, float* __restrict__ dst, size_t stride)
+__global__ void __launch_bounds__(256)
+k_cone_window(int W, int H, float maxz, int r, const ConeSpec* __restrict__ specs,
+              const float* __restrict__ src, float* __restrict__ dst, size_t stride)
 {
+    extern __shared__ float span[];
     const ConeSpec c = specs[blockIdx.y];
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)W * H) return;
-    const int x = (int)(i % W), y = (int)(i / W);
     const float* in = src + stride * blockIdx.y;
+    float* out = dst + stride * blockIdx.y;
     // window in unsigned offsets [-(r + a + b), r], mirrored into grid offsets
     const int back = r + (PASS == 0 ? c.ax + c.bx : c.ay + c.by);
     const int s = PASS == 0 ? c.sx : c.sy;
     const int lo = s > 0 ? -back : -r, hi = s > 0 ? r : back;
-    const int pos = PASS == 0 ? x : y, len = PASS == 0 ? W : H;
-    // the window's near end (unsigned offset -(r + a + b)) must lie inside
-    const bool open = s > 0 ? pos + lo < 0 : pos + hi > len - 1;
-    const int b0 = max(pos + lo, 0), b1 = min(pos + hi, len - 1);
-    float m = open ? __int_as_float(0x7f800000) : -__int_as_float(0x7f800000);
-    for (int q = open ? b1 + 1 : b0; q <= b1; ++q)
-        m = fmaxf(m, in[PASS == 0 ? pad_index(q, y, W) : pad_index(x, q, W)]);
-    dst[stride * blockIdx.y + pad_index(x, y, W)] = PASS == 0 ? m : fminf(maxz, m);
+    const int width = hi - lo + 1;
+    const float ninf = -__int_as_float(0x7f800000), pinf = __int_as_float(0x7f800000);
+    if (PASS == 0) {
+        const int segs = (W + kWinRow - 1) / kWinRow;
+        const int y = (int)(blockIdx.x / segs), x0 = (int)(blockIdx.x % segs) * kWinRow;
+        const int n = kWinRow + width - 1;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int q = x0 + lo + j;
+            span[j] = (q >= 0 && q < W) ? in[pad_index(q, y, W)] : ninf;
+        }
+        __syncthreads();
+        const int x = x0 + (int)threadIdx.x;
+        if (x >= W) return;
+        // the window's near end (unsigned offset -(r + a + b)) must lie inside
+        const bool open = s > 0 ? x + lo < 0 : x + hi > W - 1;
+        float m = open ? pinf : ninf;
+        if (!open)
+            for (int j = 0; j < width; ++j) m = fmaxf(m, span[threadIdx.x + j]);
+        out[pad_index(x, y, W)] = m;
+    } else {
+        const int cols = (W + kWinCols - 1) / kWinCols;
+        const int x0 = (int)(blockIdx.x % cols) * kWinCols, y0 = (int)(blockIdx.x / cols) * kWinRows;
+        const int tx = threadIdx.x % kWinCols, ty = threadIdx.x / kWinCols;
+        const int x = x0 + tx;
+        const int rows = kWinRows + width - 1;
+        for (int j = ty; j < rows; j += blockDim.x / kWinCols) {
+            const int q = y0 + lo + j;
+            span[j * kWinCols + tx] = (x < W && q >= 0 && q < H) ? in[pad_index(x, q, W)] : ninf;
+        }
+        __syncthreads();
+        if (x >= W) return;
+        for (int k = 0; k < kWinRowsPerThread; ++k) {
+            const int yl = ty * kWinRowsPerThread + k, y = y0 + yl;
+            if (y >= H) break;
+            const bool open = s > 0 ? y + lo < 0 : y + hi > H - 1;
+            float m = open ? pinf : ninf;
+            if (!open)
+                for (int j = 0; j < width; ++j) m = fmaxf(m, span[(yl + j) * kWinCols + tx]);
+            out[pad_index(x, y, W)] = fminf(maxz, m);
+        }
+    }
 }
 
 // The border cells of every table: +inf (a ray there stops on the height
@@ -142,15 +186,20 @@ cudaError_t launch_cone_tables(const float* grid, int W, int H, float maxz, cons
                                float* tabs, float* tmp, size_t stride, cudaStream_t st)
 {
     if (W <= 0 || H <= 0 || n_specs <= 0) return cudaSuccess;
-    const unsigned cells = (unsigned)(((long long)W * H + 255) / 256);
     const unsigned border = (unsigned)((2LL * (W + 2 + H) + 255) / 256);
     // start cells of a line family: at most kConeOrder (W + H)
     const unsigned lines = (unsigned)(((long long)kConeOrder * (W + H) + 255) / 256);
     const int r = cone_window_radius(W, H);
     k_cone_lines<0><<<dim3(lines, n_specs), 256, 0, st>>>(grid, W, H, specs, tmp, stride);
     k_cone_lines<1><<<dim3(lines, n_specs), 256, 0, st>>>(tmp, W, H, specs, tabs, stride);
-    k_cone_window<0><<<dim3(cells, n_specs), 256, 0, st>>>(W, H, maxz, r, specs, tabs, tmp, stride);
-    k_cone_window<1><<<dim3(cells, n_specs), 256, 0, st>>>(W, H, maxz, r, specs, tmp, tabs, stride);
+    // the widest window: r on one side, r + a + b (components <= kConeOrder each) on the other
+    const int wmax = 2 * r + 2 * kConeOrder + 1;
+    const unsigned win0 = (unsigned)(((long long)W + kWinRow - 1) / kWinRow * H);
+    const unsigned win1 = (unsigned)(((long long)W + kWinCols - 1) / kWinCols * ((H + kWinRows - 1) / kWinRows));
+    k_cone_window<0><<<dim3(win0, n_specs), 256, sizeof(float) * (kWinRow + wmax), st>>>(W, H, maxz, r, specs,
+                                                                                       tabs, tmp, stride);
+    k_cone_window<1><<<dim3(win1, n_specs), 256, sizeof(float) * kWinCols * (kWinRows + wmax), st>>>(
+        W, H, maxz, r, specs, tmp, tabs, stride);
     k_cone_border<<<dim3(border, n_specs), 256, 0, st>>>(W, H, tabs, stride);
     return cudaGetLastError();
 }
