@@ -265,6 +265,41 @@ def gpu_sample_lists(ranges, get) -> dict:
     return res
 
 
+def lists_vs_reference(O, scene, r: dict) -> dict:
+    """Every voxel's CSR ids, ba-RLE bytes and shadow bits against the
+    reference's own viewshed stage (include/cuda/viewshed_stage.cuh:37-125 with
+    src/cuda/kernels/viewshed_kernels.cu:7-59, rebuilt from its sources for
+    sm_100a), run after the timed region.  Never raises: a failure is
+    recorded in the key."""
+    try:
+        if O.ref_gpu() is None:
+            return {"result": "unavailable", "why": "reference CUDA pipeline not built (oracle/_ref)"}
+        ref = O.ref_stage1(scene)
+        res = {"voxels": int(scene.num_total), "neighbor_ids": int(r["csr_off"][-1]),
+               "reference": "the reference's viewshed stage rebuilt for sm_100a from its sources"}
+        first = None
+        if not np.array_equal(r["csr_off"], ref["csr_off"]):
+            first = int(np.flatnonzero(np.diff(r["csr_off"]) != np.diff(ref["csr_off"]))[0])
+        elif not np.array_equal(r["csr_ids"], ref["csr_ids"]):
+            k = int(np.flatnonzero(r["csr_ids"] != ref["csr_ids"])[0])
+            first = int(np.searchsorted(r["csr_off"], k, side="right") - 1)
+        elif not np.array_equal(r["barle_off"], ref["barle_off"]):
+            first = int(np.flatnonzero(np.diff(r["barle_off"]) != np.diff(ref["barle_off"]))[0])
+        elif not np.array_equal(r["barle"], ref["barle"]):
+            k = int(np.flatnonzero(r["barle"] != ref["barle"])[0])
+            first = int(np.searchsorted(r["barle_off"], k, side="right") - 1)
+        else:
+            sh = O.svf_to_words32(ref["svf"], r["shadow_words"])
+            if not np.array_equal(r["shadow"], sh):
+                first = int(np.flatnonzero((r["shadow"] != sh).any(axis=1))[0])
+        res["result"] = "bit-exact" if first is None else "DIFFERENT"
+        if first is not None:
+            res["first_differing_voxel"] = first
+        return res
+    except Exception as e:   # a checker, not the measurement: keep the line
+        return {"result": "unavailable", "why": f"{type(e).__name__}: {e}"[:300]}
+
+
 def list_parity(O, orc, gs: dict, cell_shadow_gpu: np.ndarray, smp: np.ndarray) -> dict:
     """Bit-exact comparison of the GPU's neighbor lists (CSR ids, ba-RLE bytes)
     and shadow words with the oracle's own traces of the same voxels, and of
@@ -748,6 +783,7 @@ def run_ours(args, world, rank, local, pg):
         extra["error_vs_fp64"] = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),
                                   "oracle": "FP64 annual-sum form over every voxel, on the GPU-built neighbor lists "
                                             "and shadow bits (those are checked by list_parity on the sample)"}
+        extra["lists_vs_reference"] = lists_vs_reference(O, scene, r)
         del r
     if rank == 0:
         # caller-side voxelization of the heightmap: the reference's host
@@ -817,7 +853,9 @@ def run_ours(args, world, rank, local, pg):
             if steps_per_ray is not None:
                 st1.update({"dda_steps_per_ray": round(steps_per_ray, 3),
                             "dda_steps_per_s": steps_per_ray * rays / t_trace,
-                            "steps_source": f"mean DDA steps per ray counted by the oracle on {nst} random voxels"})
+                            "steps_source": f"mean DDA steps per ray of the reference's loop, counted by the oracle "
+                                            f"on {nst} random voxels (upper rays above their cone's bound end "
+                                            f"early here, so fewer steps run)"})
             line["stage1"] = st1
         line.update(extra)
         print(json.dumps(line), flush=True)
