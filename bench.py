@@ -274,7 +274,8 @@ def lists_vs_reference(O, scene, r: dict) -> dict:
     try:
         if O.ref_gpu() is None:
             return {"result": "unavailable", "why": "reference CUDA pipeline not built (oracle/_ref)"}
-        ref = O.ref_stage1(scene)
+        with quiet_stdout():   # the reference stage prints its chunking from C++
+            ref = O.ref_stage1(scene)
         res = {"voxels": int(scene.num_total), "neighbor_ids": int(r["csr_off"][-1]),
                "reference": "the reference's viewshed stage rebuilt for sm_100a from its sources"}
         first = None
@@ -874,6 +875,11 @@ class quiet_stdout:
         os.dup2(self.null, 1)
 
     def __exit__(self, *a):
+        try:   # C stdio may still hold what was printed: let it go to /dev/null too
+            import ctypes
+            ctypes.CDLL(None).fflush(None)
+        except OSError:
+            pass
         os.dup2(self.saved, 1)
         os.close(self.saved)
         os.close(self.null)
