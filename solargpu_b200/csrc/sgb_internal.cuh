@@ -19,7 +19,7 @@ enum DeviceError : int {
     kErrHashFull = 2,      // a dedupe hash probe exceeded its bound
     kErrListCapacity = 4,  // a neighbor list exceeded the buffer capacity
     kErrWaitTimeout = 8,   // a bounded wait on a shared-memory barrier expired
-    kErrTraceBounds = 16,  // a ray passed the tracer's border (the index check ended it)
+    kErrTraceBounds = 16,  // a ray passed the tracer's border (its clamped index ended it)
 };
 
 // One traced direction; host-computed exactly as the reference computes Cdir
