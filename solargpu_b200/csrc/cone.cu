@@ -9,8 +9,11 @@
 //     bound[cell] = min(maxz, max of the heights of every cell a ray of the
 //                   group can visit from `cell` on),
 //
-// and the tracer ends an upward ray with no hit when its height at the cell
-// it is about to test exceeds `bound` (it checks every few steps).  The result is the reference's, bit for bit:
+// and the tracer ends an upward ray with no hit when its height exceeds the
+// bound of a cell it has reached (it loads the bound of the cell a group of
+// steps starts on and compares it with the height at the group's end, every
+// cell after that being reachable from the first).  The result is the
+// reference's, bit for bit:
 //   * upward rays only rise (t never decreases, cz > 0, and the fused
 //     multiply-add is monotone in t), so every later height test compares a
 //     cell height <= bound with a ray height > bound and fails;
